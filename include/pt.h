@@ -1,0 +1,187 @@
+/*
+ * libpt-b200: perturbative-triples energy corrections on NVIDIA B200.
+ *
+ * Drop-in for the reference's C API (ilyak/libpt src/pt.h): the eleven
+ * entry points below keep the reference's names, argument order, tensor
+ * layouts ("last index fastest", properly (anti-)symmetrised blocks) and
+ * return convention.  Arrays are HOST pointers, exactly as in the reference;
+ * the library copies them to the current CUDA device, computes there, and
+ * returns the energy.  The routines print a message and abort() on a CUDA
+ * error (the reference exits on allocation failure, src/pt.c:208-209).
+ *
+ * The device-pointer twins (libpt_*_dev) take the same tensors already in
+ * device memory, run on a caller-supplied stream, never abort, and return a
+ * status code (LIBPT_OK ...); the energy is written to *e_out.
+ *
+ * The plan API (libpt_plan_*) keeps one solve's operands resident on the
+ * device so that a caller can run the triples queue in pieces (benchmarks,
+ * serving loops) and sum the pieces itself.
+ */
+#ifndef LIBPT_B200_PT_H
+#define LIBPT_B200_PT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- reference API (src/pt.h:26-178) ------------------------------------ */
+
+/* Replaces src/pt.h:26-27 (src/misc.c:25-31). */
+void libpt_print_banner(void);
+
+/* Replaces src/pt.h:29-31 (src/misc.c:33-39).  The hook allocates the
+ * library's host-side staging memory; NULL restores malloc. */
+void libpt_set_malloc(void *(*fn)(size_t));
+
+/* Replaces src/pt.h:33-35 (src/misc.c:41-47).  NULL restores free. */
+void libpt_set_free(void (*fn)(void *));
+
+/* Replaces src/pt.h:64-66 (src/pt.c:454-479): restricted CCSD(T). */
+double libpt_rpt(size_t oa, size_t va, const double *d_ov, const double *f_ov,
+    const double *t1, const double *t2, const double *i_oovo,
+    const double *i_oovv, const double *i_ovvv);
+
+/* Replaces src/pt.h:69-71 (src/ptmp.c:455): FP32 tensors, FP64 result. */
+double libpt_rpt_mp(size_t oa, size_t va, const float *d_ov, const float *f_ov,
+    const float *t1, const float *t2, const float *i_oovo,
+    const float *i_oovv, const float *i_ovvv);
+
+/* Replaces src/pt.h:105-107 (src/pt.c:481-535): unrestricted CCSD(T). */
+double libpt_upt(size_t oa, size_t va, size_t ob, size_t vb, const double *d_ov,
+    const double *f_ov, const double *t1, const double *t2,
+    const double *i_oovo, const double *i_oovv, const double *i_ovvv);
+
+/* Replaces src/pt.h:110-112 (src/ptmp.c:482). */
+double libpt_upt_mp(size_t oa, size_t va, size_t ob, size_t vb,
+    const float *d_ov, const float *f_ov, const float *t1, const float *t2,
+    const float *i_oovo, const float *i_oovv, const float *i_ovvv);
+
+/* Replaces src/pt.h:136-139 (src/pt.c:936-972): restricted EOM-CCSD(fT). */
+double libpt_rft(size_t oa, size_t va, const double *d_ov, const double *f2_ov,
+    const double *l1, const double *t2, const double *l2, const double *i_oovv,
+    const double *i2_t2f2_oovo, const double *i3_ovvv, const double *i6_oovo,
+    const double *i7_ovvv);
+
+/* Replaces src/pt.h:142-145 (src/ptmp.c:937). */
+double libpt_rft_mp(size_t oa, size_t va, const float *d_ov, const float *f2_ov,
+    const float *l1, const float *t2, const float *l2, const float *i_oovv,
+    const float *i2_t2f2_oovo, const float *i3_ovvv, const float *i6_oovo,
+    const float *i7_ovvv);
+
+/* Replaces src/pt.h:169-172 (src/pt.c:974-1050): unrestricted EOM-CCSD(fT). */
+double libpt_uft(size_t oa, size_t va, size_t ob, size_t vb, const double *d_ov,
+    const double *f2_ov, const double *l1, const double *t2, const double *l2,
+    const double *i_oovv, const double *i2_t2f2_oovo, const double *i3_ovvv,
+    const double *i6_oovo, const double *i7_ovvv);
+
+/* Replaces src/pt.h:175-178 (src/ptmp.c:975). */
+double libpt_uft_mp(size_t oa, size_t va, size_t ob, size_t vb,
+    const float *d_ov, const float *f2_ov, const float *l1, const float *t2,
+    const float *l2, const float *i_oovv, const float *i2_t2f2_oovo,
+    const float *i3_ovvv, const float *i6_oovo, const float *i7_ovvv);
+
+/* ---- status codes ------------------------------------------------------- */
+
+#define LIBPT_OK             0
+#define LIBPT_ERR_ARG        1   /* bad size, NULL pointer, unknown option  */
+#define LIBPT_ERR_NOMEM      2   /* device or host allocation failed        */
+#define LIBPT_ERR_CUDA       3   /* a CUDA runtime/driver call failed       */
+#define LIBPT_ERR_TIMEOUT    4   /* a device-side wait ran out of its limit */
+#define LIBPT_ERR_UNSUPPORTED 5  /* option not available on this device     */
+
+/* Text of the last error on the calling thread ("" if none). */
+const char *libpt_last_error(void);
+
+/* ---- precision modes ---------------------------------------------------- */
+
+#define LIBPT_PREC_FP64   0   /* FP64 DMMA tensor-core contractions          */
+
+/* ---- device-pointer twins ----------------------------------------------
+ * Same arguments as the reference entry points, but every tensor is a
+ * device pointer on the current device and `stream` (a cudaStream_t, may be
+ * NULL for the legacy default stream) orders the work.  The call returns
+ * when the energy is known.  Scratch memory is allocated with cudaMalloc and
+ * released before return.  The *_mp twins take float tensors. */
+
+int libpt_rpt_dev(size_t oa, size_t va, const double *d_ov,
+    const double *f_ov, const double *t1, const double *t2,
+    const double *i_oovo, const double *i_oovv, const double *i_ovvv,
+    void *stream, double *e_out);
+int libpt_upt_dev(size_t oa, size_t va, size_t ob, size_t vb,
+    const double *d_ov, const double *f_ov, const double *t1, const double *t2,
+    const double *i_oovo, const double *i_oovv, const double *i_ovvv,
+    void *stream, double *e_out);
+int libpt_rft_dev(size_t oa, size_t va, const double *d_ov,
+    const double *f2_ov, const double *l1, const double *t2, const double *l2,
+    const double *i_oovv, const double *i2_t2f2_oovo, const double *i3_ovvv,
+    const double *i6_oovo, const double *i7_ovvv, void *stream,
+    double *e_out);
+int libpt_uft_dev(size_t oa, size_t va, size_t ob, size_t vb,
+    const double *d_ov, const double *f2_ov, const double *l1,
+    const double *t2, const double *l2, const double *i_oovv,
+    const double *i2_t2f2_oovo, const double *i3_ovvv, const double *i6_oovo,
+    const double *i7_ovvv, void *stream, double *e_out);
+
+int libpt_rpt_mp_dev(size_t oa, size_t va, const float *d_ov,
+    const float *f_ov, const float *t1, const float *t2, const float *i_oovo,
+    const float *i_oovv, const float *i_ovvv, void *stream, double *e_out);
+int libpt_upt_mp_dev(size_t oa, size_t va, size_t ob, size_t vb,
+    const float *d_ov, const float *f_ov, const float *t1, const float *t2,
+    const float *i_oovo, const float *i_oovv, const float *i_ovvv,
+    void *stream, double *e_out);
+int libpt_rft_mp_dev(size_t oa, size_t va, const float *d_ov,
+    const float *f2_ov, const float *l1, const float *t2, const float *l2,
+    const float *i_oovv, const float *i2_t2f2_oovo, const float *i3_ovvv,
+    const float *i6_oovo, const float *i7_ovvv, void *stream, double *e_out);
+int libpt_uft_mp_dev(size_t oa, size_t va, size_t ob, size_t vb,
+    const float *d_ov, const float *f2_ov, const float *l1, const float *t2,
+    const float *l2, const float *i_oovv, const float *i2_t2f2_oovo,
+    const float *i3_ovvv, const float *i6_oovo, const float *i7_ovvv,
+    void *stream, double *e_out);
+
+/* ---- plans: resident operands, the triples queue run in pieces ----------
+ *
+ * A plan holds one solve's operands on the device in the library's padded
+ * layout.  Its triples queue lists, in order, the same-spin triples i<j<k of
+ * the alpha case, those of the beta case (unrestricted only), the mixed-spin
+ * triples i<j (alpha), k (beta), and those of the beta-beta-alpha case
+ * (unrestricted only) -- the order of src/pt.c:514-529.  Running every queue
+ * entry once and calling libpt_plan_energy gives the solver's result
+ * (including the restricted factor 2, src/pt.c:478).
+ *
+ * kind: 0 = (T) restricted, 1 = (T) unrestricted, 2 = (fT) restricted,
+ *       3 = (fT) unrestricted.
+ * args: the pt.h tensor pointers of that kind, in the reference's argument
+ *       order (7 for (T), 10 for (fT)), DEVICE pointers, FP64 (dtype 0) or
+ *       FP32 (dtype 1).  They are read during libpt_plan_create only. */
+typedef struct libpt_plan libpt_plan;
+
+int libpt_plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
+    const void *const *args, int dtype, int precision, void *stream,
+    libpt_plan **out);
+/* Number of entries of the triples queue. */
+int64_t libpt_plan_queue_length(const libpt_plan *plan);
+/* Algorithmic flops of queue entries [first, first+n): twice the
+ * multiply-adds of the reference's own contractions for those triples. */
+double libpt_plan_flops(const libpt_plan *plan, int64_t first, int64_t n);
+/* Compute queue entries idx[0..n) (host array); their energies are stored
+ * in the plan (overwriting earlier runs of the same entries).  Asynchronous
+ * on the plan's stream. */
+int libpt_plan_run(libpt_plan *plan, const int64_t *idx, size_t n);
+/* Compute every queue entry (the whole solve).  Asynchronous. */
+int libpt_plan_run_all(libpt_plan *plan);
+/* Wait for the plan's stream and return the fixed-order, compensated sum of
+ * the stored energies of entries idx[0..n) (idx == NULL: all entries),
+ * scaled by the restricted factor when the whole queue is summed. */
+int libpt_plan_energy(libpt_plan *plan, const int64_t *idx, size_t n,
+    double *e_out);
+int libpt_plan_destroy(libpt_plan *plan);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* LIBPT_B200_PT_H */

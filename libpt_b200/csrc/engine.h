@@ -1,0 +1,105 @@
+// Host/device shared structures of the triples engine.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ptb {
+
+// ---- FP64 DMMA GEMM ------------------------------------------------------
+//
+// One "job" is C[M][N] = sum over segments s of (+/-) A_s B_s for one
+// triple, where A_s is a [rows][K_s] slice of a padded amplitude/OOVO block
+// (TMA view: dims (K, rows, Q, P)) and B_s a [K_s][N] slice of a padded
+// OVVV/amplitude block (TMA view: dims (N, K, P)).  The slices are selected
+// by the occupied indices (Q, P) resp. (P) of the triple.
+
+constexpr int GEMM_BM = 128;   // rows of a CTA tile
+constexpr int GEMM_BN = 128;   // columns of a CTA tile
+constexpr int GEMM_BK = 16;    // contraction depth of one pipeline stage
+constexpr int GEMM_STAGES = 5;
+constexpr int GEMM_CONSUMER_WARPS = 8;
+constexpr int GEMM_THREADS = (GEMM_CONSUMER_WARPS + 1) * 32;
+constexpr int MAX_SEG = 6;
+constexpr int MAX_MAPS = 24;
+
+struct GemmSeg {
+  int16_t amap, bmap;   // indices into MapSet
+  int16_t neg, pad_;    // neg != 0: subtract this product
+  int32_t a_q, a_p;     // A-view coordinates of dims 2 and 3
+  int32_t b_p;          // B-view coordinate of dim 2
+  int32_t ksteps;       // ceil(K_s / GEMM_BK)
+};
+
+struct GemmJob {
+  double *out;          // C, row-major with leading dimension ldc
+  int64_t ldc;
+  int32_t M, N;         // N <= ldc, N % 4 == 0
+  int32_t ntiles_n;     // ceil(N / GEMM_BN)
+  int32_t tile_begin;   // first flat tile index of this job in the launch
+  int32_t nseg, pad_;
+  GemmSeg seg[MAX_SEG];
+};
+
+struct MapSet {
+  CUtensorMap m[MAX_MAPS];
+};
+
+size_t gemm_smem_bytes();
+cudaError_t gemm_dmma_launch(const MapSet &maps, const GemmJob *d_jobs,
+                             int njobs, int total_tiles, unsigned *d_err,
+                             cudaStream_t st);
+
+// ---- energy epilogues ------------------------------------------------------
+
+constexpr int EPI_A = 8, EPI_B = 8, EPI_C = 32;   // tile extents a x b x c
+constexpr int EPI_THREADS = 256;
+constexpr int EPI_PAD = EPI_B + 1;                // smem row pad (banks)
+
+// Arguments shared by the same-spin (aaa) and mixed-spin (aab) epilogues.
+struct EpiArgs {
+  const double *ws;       // triple t's arrays start at ws + t * ws_stride
+  int64_t ws_stride;
+  int64_t offL[3];        // array offsets of the (first) amplitude W / L
+  int64_t offR[3];        // offsets of R for (fT); offR[0] < 0 for (T)
+  int64_t ld[3];          // leading dims: aaa {ldT}; aab {ldU1, ldU2, ldP}
+  int64_t rowU1, rowU2;   // aab: padded inner extents of U1 (vb) and U2 (va)
+  const int *trip;        // i, j, k per triple of the batch
+  int oa, va, ob, vb;
+  const double *d_a, *d_b;                  // denominators [o][v]
+  const double *ov1_a, *ov1_b;              // t1 / l1
+  const double *g1_ab, *g1_aa;              // i_oovv blocks
+  int64_t g1_ld_ab, g1_ld_aa;               // their inner leading dims
+  const double *ov2_a, *ov2_b;              // f_ov / f2_ov
+  const double *g2_ab, *g2_aa;              // t2 / l2 blocks
+  int64_t g2_ld_ab, g2_ld_aa;
+  double *partials;       // [ntrip][ntiles]
+  int ntiles;
+  const int4 *tiles;      // aaa: (a0, b0, c0); aab: (a0, b0, 0) block pairs
+  int ctiles;             // aab: number of c blocks
+};
+
+size_t epi_smem_bytes(bool aab, bool ft);
+cudaError_t epi_aaa_launch(const EpiArgs &a, bool ft, int ntrip,
+                           cudaStream_t st);
+cudaError_t epi_aab_launch(const EpiArgs &a, bool ft, int ntrip,
+                           cudaStream_t st);
+// e_slot[slot[t]] = fixed-order sum of partials[t][0..ntiles).
+cudaError_t reduce_partials_launch(const double *partials, int ntiles,
+                                   int ntrip, const int *slot, double *e_slot,
+                                   cudaStream_t st);
+
+// ---- operand preparation ---------------------------------------------------
+
+// dst[r][c] = src[r][c] (c < w), 0 (w <= c < dpitch); converts FP32 to FP64.
+cudaError_t repack_launch(const void *src, bool src_fp32, double *dst,
+                          int64_t rows, int64_t w, int64_t dpitch,
+                          cudaStream_t st);
+// out[p][q][pair(a,b)] = tau[p][q][a][b] for a > b (pair = a(a-1)/2 + b);
+// tau rows padded to ldv, out rows padded to ldp (zero fill).
+cudaError_t pack_pairs_launch(const double *tau, double *out, int64_t npq,
+                              int v, int64_t ldv, int64_t ldp,
+                              cudaStream_t st);
+
+}  // namespace ptb

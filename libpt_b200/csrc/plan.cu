@@ -1,0 +1,791 @@
+// The triples engine: operand preparation, spin cases, job templates and the
+// batched run over the triples queue.
+//
+// Reference structure restated here:
+//   spin-block split of the packed arguments   src/pt.c:460-467, 487-512,
+//                                              943-956, 981-1021
+//   spin cases and their block roles           src/pt.c:469-473, 514-529,
+//                                              958-966, 1023-1044
+//   triple enumeration (i<j<k; i<j, all k)     src/pt.c:210-221, 333-344
+//   restricted factor 2                        src/pt.c:478, 971
+// The reference's OpenMP/MPI distribution of triples (src/pt.c:197-229)
+// becomes batches of triples, each batch one GEMM launch over all of its
+// triples' output tiles and one epilogue launch; per-triple energies land in
+// slots indexed by queue position and are summed in queue order.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "plan.h"
+#include "pt.h"
+
+namespace ptb {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string &msg) { g_last_error = msg; }
+const char *last_error() { return g_last_error.c_str(); }
+
+namespace {
+
+int64_t pad4(int64_t x) { return (x + 3) & ~int64_t(3); }
+int64_t pad32(int64_t x) { return (x + 31) & ~int64_t(31); }
+int64_t npair(int64_t v) { return v * (v - 1) / 2; }
+int ksteps(int64_t k) { return (int)((k + GEMM_BK - 1) / GEMM_BK); }
+
+#define CK(call)                                                          \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess) {                                              \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));      \
+      return e_ == cudaErrorMemoryAllocation ? LIBPT_ERR_NOMEM            \
+                                             : LIBPT_ERR_CUDA;            \
+    }                                                                     \
+  } while (0)
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType,
+                                  cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p,
+                                cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// A-view of a padded block [P][Q][R][Kpad] with logical K: dims (K, R, Q, P),
+// box (4, GEMM_BM, 1, 1).
+int map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R, int64_t Q,
+          int64_t P) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return LIBPT_ERR_CUDA;
+  }
+  const int64_t kp = pad4(K);
+  cuuint64_t dims[4] = {(cuuint64_t)std::max<int64_t>(K, 1),
+                        (cuuint64_t)std::max<int64_t>(R, 1),
+                        (cuuint64_t)std::max<int64_t>(Q, 1),
+                        (cuuint64_t)std::max<int64_t>(P, 1)};
+  cuuint64_t strides[3] = {(cuuint64_t)(kp * 8), (cuuint64_t)(R * kp * 8),
+                           (cuuint64_t)(Q * R * kp * 8)};
+  cuuint32_t box[4] = {4, (cuuint32_t)GEMM_BM, 1, 1};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)p, dims,
+                   strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (A view) failed: " + std::to_string(r));
+    return LIBPT_ERR_CUDA;
+  }
+  return LIBPT_OK;
+}
+
+// B-view of a padded block [P][K][Nld] with logical N: dims (N, K, P),
+// box (4, GEMM_BK, 1).
+int map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld, int64_t K,
+          int64_t P) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return LIBPT_ERR_CUDA;
+  }
+  cuuint64_t dims[3] = {(cuuint64_t)std::max<int64_t>(N, 1),
+                        (cuuint64_t)std::max<int64_t>(K, 1),
+                        (cuuint64_t)std::max<int64_t>(P, 1)};
+  cuuint64_t strides[2] = {(cuuint64_t)(Nld * 8), (cuuint64_t)(K * Nld * 8)};
+  cuuint32_t box[3] = {4, (cuuint32_t)GEMM_BK, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)p, dims,
+                   strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (B view) failed: " + std::to_string(r));
+    return LIBPT_ERR_CUDA;
+  }
+  return LIBPT_OK;
+}
+
+int dalloc(libpt_plan *p, void **ptr, size_t bytes) {
+  *ptr = nullptr;
+  if (bytes == 0) bytes = 256;
+  cudaError_t e = cudaMalloc(ptr, bytes);
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc(" + std::to_string(bytes) +
+              " bytes): " + cudaGetErrorString(e));
+    cudaGetLastError();
+    return LIBPT_ERR_NOMEM;
+  }
+  p->allocs.push_back(*ptr);
+  return LIBPT_OK;
+}
+
+// Copies rows x w elements (FP64 or FP32, host or device) into a padded FP64
+// device block rows x dpitch.  Host sources go through a device staging
+// buffer in chunks.
+struct Uploader {
+  libpt_plan *p;
+  bool host, fp32;
+  void *stage = nullptr;
+  size_t stage_bytes = 0;
+
+  int put(double *dst, const void *src, int64_t rows, int64_t w,
+          int64_t dpitch) {
+    if (rows <= 0 || dpitch <= 0) return LIBPT_OK;
+    const size_t es = fp32 ? 4 : 8;
+    if (!host) {
+      if (w == dpitch && !fp32)
+        CK(cudaMemcpyAsync(dst, src, (size_t)rows * w * 8,
+                           cudaMemcpyDeviceToDevice, p->st));
+      else
+        CK(repack_launch(src, fp32, dst, rows, w, dpitch, p->st));
+      return LIBPT_OK;
+    }
+    if (!stage) {
+      stage_bytes = (size_t)256 << 20;
+      if (dalloc(p, &stage, stage_bytes)) return LIBPT_ERR_NOMEM;
+    }
+    if (w == dpitch) {   // unpadded: copy as a flat array
+      const int64_t total = rows * w, chunk = (int64_t)(stage_bytes / es);
+      for (int64_t x0 = 0; x0 < total; x0 += chunk) {
+        const int64_t nx = std::min(chunk, total - x0);
+        CK(cudaMemcpyAsync(stage, (const char *)src + (size_t)x0 * es,
+                           (size_t)nx * es, cudaMemcpyHostToDevice, p->st));
+        CK(repack_launch(stage, fp32, dst + x0, 1, nx, nx, p->st));
+      }
+      return LIBPT_OK;
+    }
+    const int64_t chunk =
+        std::max<int64_t>(1, (int64_t)(stage_bytes / (es * std::max<int64_t>(w, 1))));
+    for (int64_t r0 = 0; r0 < rows; r0 += chunk) {
+      const int64_t nr = std::min(chunk, rows - r0);
+      CK(cudaMemcpyAsync(stage, (const char *)src + (size_t)r0 * w * es,
+                         (size_t)nr * w * es, cudaMemcpyHostToDevice, p->st));
+      CK(repack_launch(stage, fp32, dst + r0 * dpitch, nr, w, dpitch, p->st));
+    }
+    return LIBPT_OK;
+  }
+};
+
+// Element counts of the four spin blocks of each tensor family.
+struct Sizes {
+  int64_t oa, va, ob, vb;
+  int64_t oovv(int b) const {
+    return b == 0 ? oa * oa * va * va : b == 1 ? oa * ob * va * vb
+         : b == 2 ? ob * ob * vb * vb : ob * oa * vb * va;
+  }
+  int64_t oovo(int b) const {
+    return b == 0 ? oa * oa * va * oa : b == 1 ? oa * ob * va * ob
+         : b == 2 ? ob * ob * vb * ob : ob * oa * vb * oa;
+  }
+  int64_t ovvv(int b) const {
+    return b == 0 ? oa * va * npair(va) : b == 1 ? oa * vb * va * vb
+         : b == 2 ? ob * vb * npair(vb) : ob * va * vb * va;
+  }
+  // (rows, inner width) of each block in pt.h layout
+  void tau_shape(int b, int64_t &rows, int64_t &w) const {
+    rows = b == 0 ? oa * oa * va : b == 1 ? oa * ob * va
+         : b == 2 ? ob * ob * vb : ob * oa * vb;
+    w = (b == 0 || b == 3) ? va : vb;
+  }
+  void oovo_shape(int b, int64_t &rows, int64_t &w) const {
+    rows = b == 0 ? oa * oa * va : b == 1 ? oa * ob * va
+         : b == 2 ? ob * ob * vb : ob * oa * vb;
+    w = (b == 0 || b == 3) ? oa : ob;
+  }
+  void ovvv_shape(int b, int64_t &rows, int64_t &w) const {
+    rows = b == 0 ? oa * va : b == 1 ? oa * vb * va
+         : b == 2 ? ob * vb : ob * va * vb;
+    w = b == 0 ? npair(va) : b == 1 ? vb : b == 2 ? npair(vb) : va;
+  }
+};
+
+// Upload one amplitude + integrals set into padded blocks.
+int upload_set(libpt_plan *p, Uploader &up, const Sizes &S, OperandSet &set,
+               const void *tau, const void *oovo, const void *ovvv) {
+  const int nb = p->unrestricted ? 4 : 2;
+  const size_t es = p->dtype ? 4 : 8;
+  int64_t off_t = 0, off_o = 0, off_v = 0;
+  for (int b = 0; b < nb; ++b) {
+    int64_t rows, w;
+    S.tau_shape(b, rows, w);
+    if (dalloc(p, (void **)&set.tau[b], rows * pad4(w) * 8)) return LIBPT_ERR_NOMEM;
+    if (int r = up.put(set.tau[b], (const char *)tau + off_t * es, rows, w, pad4(w)))
+      return r;
+    off_t += S.oovv(b);
+    S.oovo_shape(b, rows, w);
+    if (dalloc(p, (void **)&set.oovo[b], rows * pad4(w) * 8)) return LIBPT_ERR_NOMEM;
+    if (int r = up.put(set.oovo[b], (const char *)oovo + off_o * es, rows, w, pad4(w)))
+      return r;
+    off_o += S.oovo(b);
+    S.ovvv_shape(b, rows, w);
+    if (dalloc(p, (void **)&set.ovvv[b], rows * pad4(w) * 8)) return LIBPT_ERR_NOMEM;
+    if (int r = up.put(set.ovvv[b], (const char *)ovvv + off_v * es, rows, w, pad4(w)))
+      return r;
+    off_v += S.ovvv(b);
+  }
+  if (!p->unrestricted) {   // src/pt.c:471-473: baba blocks alias abab
+    set.tau[3] = set.tau[1];
+    set.oovo[3] = set.oovo[1];
+    set.ovvv[3] = set.ovvv[1];
+  }
+  // packed-pair copies of the same-spin amplitudes
+  for (int s = 0; s < (p->unrestricted ? 2 : 1); ++s) {
+    const int64_t o = s ? S.ob : S.oa, v = s ? S.vb : S.va;
+    const int64_t ldp = pad4(npair(v));
+    if (dalloc(p, (void **)&set.taup[s], o * o * ldp * 8)) return LIBPT_ERR_NOMEM;
+    CK(pack_pairs_launch(set.tau[s ? 2 : 0], set.taup[s], o * o, (int)v,
+                         pad4(v), ldp, p->st));
+  }
+  return LIBPT_OK;
+}
+
+SegT seg(int amap, int bmap, bool neg, int aq, int ap, int bp, int64_t k) {
+  SegT s;
+  s.amap = (int16_t)amap;
+  s.bmap = (int16_t)bmap;
+  s.neg = neg ? 1 : 0;
+  s.aq = (int8_t)aq;
+  s.ap = (int8_t)ap;
+  s.bp = (int8_t)bp;
+  s.ksteps = ksteps(k);
+  return s;
+}
+
+enum { I = 0, J = 1, K = 2 };
+
+// Same-spin case: four maps per operand set, one job (T) per set.
+int build_aaa(libpt_plan *p, SpinCase &c) {
+  const int s = c.flip;
+  const int64_t o = c.oa, v = c.va, np = npair(v), ldT = pad4(np);
+  const int nset = p->ft ? 2 : 1;
+  int64_t offs[2];
+  int64_t stride = 0;
+  for (int x = 0; x < nset; ++x) {
+    offs[x] = stride;
+    stride += pad32(v * ldT);
+  }
+  for (int x = 0; x < nset; ++x) {
+    const OperandSet &set = x ? p->R : p->L;
+    const int b0 = 4 * x;
+    if (int r = map_a(&c.maps.m[b0 + 0], set.tau[s ? 2 : 0], v, v, o, o)) return r;
+    if (int r = map_a(&c.maps.m[b0 + 1], set.oovo[s ? 2 : 0], o, v, o, o)) return r;
+    if (int r = map_b(&c.maps.m[b0 + 2], set.ovvv[s ? 2 : 0], np, ldT, v, o)) return r;
+    if (int r = map_b(&c.maps.m[b0 + 3], set.taup[s], np, ldT, o, o)) return r;
+    JobT j;
+    j.off = offs[x];
+    j.M = (int)v;
+    j.N = (int)ldT;
+    j.ldc = ldT;
+    j.nseg = 6;
+    // T[x][pair] = sum_d (t_ij - t_ik - t_kj)[x][d] I_(k,j,i)[d][pair]
+    //            + sum_l (O_jk - O_ik - O_ji)[x][l] tp_(i,j,k)[l][pair]
+    j.seg[0] = seg(b0 + 0, b0 + 2, false, J, I, K, v);
+    j.seg[1] = seg(b0 + 0, b0 + 2, true, K, I, J, v);
+    j.seg[2] = seg(b0 + 0, b0 + 2, true, J, K, I, v);
+    j.seg[3] = seg(b0 + 1, b0 + 3, false, K, J, I, o);
+    j.seg[4] = seg(b0 + 1, b0 + 3, true, K, I, J, o);
+    j.seg[5] = seg(b0 + 1, b0 + 3, true, I, J, K, o);
+    if (np > 0) c.jobs.push_back(j);
+  }
+  EpiArgs &e = c.epi;
+  memset(&e, 0, sizeof(e));
+  e.ws_stride = stride;
+  e.offL[0] = offs[0];
+  e.offR[0] = p->ft ? offs[1] : -1;
+  e.ld[0] = ldT;
+  e.oa = (int)o;
+  e.va = (int)v;
+  e.ob = (int)o;
+  e.vb = (int)v;
+  const int64_t ovoff = s ? (int64_t)p->oa * p->va : 0;
+  e.d_a = p->d_ov + ovoff;
+  e.ov1_a = p->ov1 + ovoff;
+  e.ov2_a = p->ov2 + ovoff;
+  e.g1_aa = p->oovv[s ? 2 : 0];
+  e.g1_ld_aa = v;
+  e.g2_aa = p->L.tau[s ? 2 : 0];
+  e.g2_ld_aa = pad4(v);
+  // tiles (a0, b0, c0) holding at least one a > b > c
+  std::vector<int4> tiles;
+  for (int64_t a0 = 0; a0 < v; a0 += EPI_A) {
+    const int64_t amax = std::min<int64_t>(a0 + EPI_A - 1, v - 1);
+    for (int64_t b0 = 0; b0 <= a0; b0 += EPI_B) {
+      if (amax - 1 < b0) continue;
+      const int64_t bmax = std::min<int64_t>(b0 + EPI_B - 1, amax - 1);
+      for (int64_t c0 = 0; c0 < bmax; c0 += EPI_C)
+        tiles.push_back(make_int4((int)a0, (int)b0, (int)c0, 0));
+    }
+  }
+  c.ntiles = (int)tiles.size();
+  c.ctiles = 1;
+  if (c.ntiles) {
+    if (dalloc(p, (void **)&c.d_tiles, tiles.size() * sizeof(int4))) return LIBPT_ERR_NOMEM;
+    CK(cudaMemcpyAsync(c.d_tiles, tiles.data(), tiles.size() * sizeof(int4),
+                       cudaMemcpyHostToDevice, p->st));
+    CK(cudaStreamSynchronize(p->st));
+  }
+  const double vv = (double)v;
+  c.flops_per_triple = 3.0 * vv * vv * vv * (vv - 1) + 6.0 * o * vv * vv * vv;
+  if (p->ft) c.flops_per_triple *= 2;
+  return LIBPT_OK;
+}
+
+// Mixed-spin case: twelve maps per operand set, three jobs (U1, U2, P).
+int build_aab(libpt_plan *p, SpinCase &c) {
+  const int f = c.flip;
+  const int64_t oa = c.oa, va = c.va, ob = c.ob, vb = c.vb;
+  const int64_t np = npair(va);
+  const int64_t ld1 = va * pad4(vb), ld2 = vb * pad4(va), ldP = pad4(np);
+  const int nset = p->ft ? 2 : 1;
+  int64_t offs[2][3];
+  int64_t stride = 0;
+  for (int x = 0; x < nset; ++x) {
+    offs[x][0] = stride;
+    stride += pad32(va * ld1);
+    offs[x][1] = stride;
+    stride += pad32(va * ld2);
+    offs[x][2] = stride;
+    stride += pad32(vb * ldP);
+  }
+  // block roles (src/pt.c:521-529): flip swaps alpha and beta
+  const int Taa = f ? 2 : 0, Tab = f ? 3 : 1, Tba = f ? 1 : 3;
+  for (int x = 0; x < nset; ++x) {
+    const OperandSet &S = x ? p->R : p->L;
+    CUtensorMap *m = &c.maps.m[12 * x];
+    int r;
+    if ((r = map_a(&m[0], S.tau[Taa], va, va, oa, oa))) return r;
+    if ((r = map_a(&m[1], S.tau[Tab], vb, va, ob, oa))) return r;
+    if ((r = map_a(&m[2], S.tau[Tba], va, vb, oa, ob))) return r;
+    if ((r = map_a(&m[3], S.oovo[Taa], oa, va, oa, oa))) return r;
+    if ((r = map_a(&m[4], S.oovo[Tab], ob, va, ob, oa))) return r;
+    if ((r = map_a(&m[5], S.oovo[Tba], oa, vb, oa, ob))) return r;
+    if ((r = map_b(&m[6], S.ovvv[Taa], np, ldP, va, oa))) return r;
+    if ((r = map_b(&m[7], S.ovvv[Tab], ld1, ld1, vb, oa))) return r;
+    if ((r = map_b(&m[8], S.ovvv[Tba], ld2, ld2, va, ob))) return r;
+    if ((r = map_b(&m[9], S.taup[f], np, ldP, oa, oa))) return r;
+    if ((r = map_b(&m[10], S.tau[Tab], ld1, ld1, ob, oa))) return r;
+    if ((r = map_b(&m[11], S.tau[Tba], ld2, ld2, oa, ob))) return r;
+    const int b = 12 * x;
+    JobT u1, u2, pp;
+    // U1[x][y,c] = -t_ik I_j + t_jk I_i + O_jk t_i - O_ik t_j
+    u1.off = offs[x][0];
+    u1.M = (int)va;
+    u1.N = (int)ld1;
+    u1.ldc = ld1;
+    u1.nseg = 4;
+    u1.seg[0] = seg(b + 1, b + 7, true, K, I, J, vb);
+    u1.seg[1] = seg(b + 1, b + 7, false, K, J, I, vb);
+    u1.seg[2] = seg(b + 4, b + 10, false, K, J, I, ob);
+    u1.seg[3] = seg(b + 4, b + 10, true, K, I, J, ob);
+    // U2[x][c,y] = -t_ij I_k + O_ji t_k
+    u2.off = offs[x][1];
+    u2.M = (int)va;
+    u2.N = (int)ld2;
+    u2.ldc = ld2;
+    u2.nseg = 2;
+    u2.seg[0] = seg(b + 0, b + 8, true, J, I, K, va);
+    u2.seg[1] = seg(b + 3, b + 11, false, I, J, K, oa);
+    // P[c][pair] = -t_kj I_i + t_ki I_j - O_kj tp_i + O_ki tp_j
+    pp.off = offs[x][2];
+    pp.M = (int)vb;
+    pp.N = (int)ldP;
+    pp.ldc = ldP;
+    pp.nseg = 4;
+    pp.seg[0] = seg(b + 2, b + 6, true, J, K, I, va);
+    pp.seg[1] = seg(b + 2, b + 6, false, I, K, J, va);
+    pp.seg[2] = seg(b + 5, b + 9, true, J, K, I, oa);
+    pp.seg[3] = seg(b + 5, b + 9, false, I, K, J, oa);
+    c.jobs.push_back(u1);
+    c.jobs.push_back(u2);
+    if (np > 0) c.jobs.push_back(pp);
+  }
+  EpiArgs &e = c.epi;
+  memset(&e, 0, sizeof(e));
+  e.ws_stride = stride;
+  for (int q = 0; q < 3; ++q) {
+    e.offL[q] = offs[0][q];
+    e.offR[q] = p->ft ? offs[1][q] : -1;
+  }
+  e.ld[0] = ld1;
+  e.ld[1] = ld2;
+  e.ld[2] = ldP;
+  e.rowU1 = pad4(vb);
+  e.rowU2 = pad4(va);
+  e.oa = (int)oa;
+  e.va = (int)va;
+  e.ob = (int)ob;
+  e.vb = (int)vb;
+  const int64_t offA = f ? (int64_t)p->oa * p->va : 0;
+  const int64_t offB = f ? 0 : (int64_t)p->oa * p->va;
+  const int64_t offB_r = p->unrestricted ? offB : 0;
+  e.d_a = p->d_ov + offA;
+  e.d_b = p->d_ov + offB_r;
+  e.ov1_a = p->ov1 + offA;
+  e.ov1_b = p->ov1 + offB_r;
+  e.ov2_a = p->ov2 + offA;
+  e.ov2_b = p->ov2 + offB_r;
+  e.g1_ab = p->oovv[Tab];
+  e.g1_ld_ab = vb;
+  e.g1_aa = p->oovv[Taa];
+  e.g1_ld_aa = va;
+  e.g2_ab = p->L.tau[Tab];
+  e.g2_ld_ab = pad4(vb);
+  e.g2_aa = p->L.tau[Taa];
+  e.g2_ld_aa = pad4(va);
+  std::vector<int4> tiles;
+  for (int64_t a0 = 0; a0 < va; a0 += EPI_A) {
+    const int64_t amax = std::min<int64_t>(a0 + EPI_A - 1, va - 1);
+    for (int64_t b0 = 0; b0 <= a0; b0 += EPI_B)
+      if (amax - 1 >= b0) tiles.push_back(make_int4((int)a0, (int)b0, 0, 0));
+  }
+  c.ctiles = (int)((vb + EPI_C - 1) / EPI_C);
+  c.ntiles = (int)tiles.size() * c.ctiles;
+  if (!tiles.empty()) {
+    if (dalloc(p, (void **)&c.d_tiles, tiles.size() * sizeof(int4))) return LIBPT_ERR_NOMEM;
+    CK(cudaMemcpyAsync(c.d_tiles, tiles.data(), tiles.size() * sizeof(int4),
+                       cudaMemcpyHostToDevice, p->st));
+    CK(cudaStreamSynchronize(p->st));
+  }
+  const double A = (double)va, B = (double)vb;
+  c.flops_per_triple = 2 * A * A * A * B + 4 * A * A * B * B +
+                       2 * B * A * A * (A - 1) + 6 * A * A * B * oa +
+                       4 * A * A * B * ob;
+  if (p->ft) c.flops_per_triple *= 2;
+  return LIBPT_OK;
+}
+
+int add_cases(libpt_plan *p) {
+  const int oa = p->oa, va = p->va, ob = p->ob, vb = p->vb;
+  auto add = [&](int type, int flip, int o1, int v1, int o2, int v2) {
+    SpinCase c;
+    c.type = type;
+    c.flip = flip;
+    c.oa = o1;
+    c.va = v1;
+    c.ob = o2;
+    c.vb = v2;
+    c.first = (int64_t)p->queue.size();
+    const int ci = (int)p->cases.size();
+    // src/pt.c:195-196, 318-319: an empty space contributes nothing
+    const bool empty = type == 0 ? (o1 == 0 || v1 == 0)
+                                 : (o1 == 0 || v1 == 0 || o2 == 0 || v2 == 0);
+    if (!empty) {
+      if (type == 0) {
+        for (int i = 0; i < o1; ++i)
+          for (int j = i + 1; j < o1; ++j)
+            for (int k = j + 1; k < o1; ++k)
+              p->queue.push_back(make_int4(ci, i, j, k));
+      } else {
+        for (int i = 0; i < o1; ++i)
+          for (int j = i + 1; j < o1; ++j)
+            for (int k = 0; k < o2; ++k)
+              p->queue.push_back(make_int4(ci, i, j, k));
+      }
+    }
+    c.count = (int64_t)p->queue.size() - c.first;
+    p->cases.push_back(c);
+  };
+  add(0, 0, oa, va, oa, va);
+  if (p->unrestricted) add(0, 1, ob, vb, ob, vb);
+  add(1, 0, oa, va, ob, vb);
+  if (p->unrestricted) add(1, 1, ob, vb, oa, va);
+  for (SpinCase &c : p->cases) {
+    if (c.count == 0) continue;
+    int r = c.type == 0 ? build_aaa(p, c) : build_aab(p, c);
+    if (r) return r;
+  }
+  return LIBPT_OK;
+}
+
+// Runs queue entries of one case, `n` at a time.
+int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
+  const size_t per = (size_t)c.epi.ws_stride * sizeof(double);
+  size_t nb = p->ws_budget / std::max<size_t>(per, 1);
+  if (p->max_batch) nb = std::min(nb, p->max_batch);
+  nb = std::max<size_t>(1, std::min<size_t>({nb, (size_t)4096, ents.size()}));
+  if (nb * per > p->ws_bytes) {
+    if (p->ws) {
+      cudaFree(p->ws);
+      p->allocs.erase(std::find(p->allocs.begin(), p->allocs.end(), (void *)p->ws));
+      p->ws = nullptr;
+    }
+    if (dalloc(p, (void **)&p->ws, nb * per)) return LIBPT_ERR_NOMEM;
+    p->ws_bytes = nb * per;
+  }
+  const size_t njt = c.jobs.size();
+  std::vector<GemmJob> jobs;
+  std::vector<int> trip, slot;
+  for (size_t b0 = 0; b0 < ents.size(); b0 += nb) {
+    const size_t n = std::min(nb, ents.size() - b0);
+    // buffers sized for this batch
+    if (n * njt > p->jobs_cap) {
+      if (dalloc(p, (void **)&p->d_jobs, n * njt * sizeof(GemmJob))) return LIBPT_ERR_NOMEM;
+      p->jobs_cap = n * njt;
+    }
+    if (n > p->trip_cap) {
+      if (dalloc(p, (void **)&p->d_trip, 3 * n * sizeof(int))) return LIBPT_ERR_NOMEM;
+      if (dalloc(p, (void **)&p->d_slot, n * sizeof(int))) return LIBPT_ERR_NOMEM;
+      p->trip_cap = n;
+    }
+    if (n * (size_t)c.ntiles > p->partials_cap) {
+      if (dalloc(p, (void **)&p->partials, n * c.ntiles * sizeof(double)))
+        return LIBPT_ERR_NOMEM;
+      p->partials_cap = n * c.ntiles;
+    }
+    jobs.clear();
+    trip.clear();
+    slot.clear();
+    int tiles = 0;
+    for (size_t t = 0; t < n; ++t) {
+      const int4 q = p->queue[ents[b0 + t]];
+      const int ijk[3] = {q.y, q.z, q.w};
+      trip.push_back(q.y);
+      trip.push_back(q.z);
+      trip.push_back(q.w);
+      slot.push_back((int)ents[b0 + t]);
+      for (const JobT &jt : c.jobs) {
+        GemmJob g;
+        memset(&g, 0, sizeof(g));
+        g.out = p->ws + (int64_t)t * c.epi.ws_stride + jt.off;
+        g.ldc = jt.ldc;
+        g.M = jt.M;
+        g.N = jt.N;
+        g.ntiles_n = (jt.N + GEMM_BN - 1) / GEMM_BN;
+        g.tile_begin = tiles;
+        g.nseg = jt.nseg;
+        for (int s = 0; s < jt.nseg; ++s) {
+          const SegT &st = jt.seg[s];
+          GemmSeg &gs = g.seg[s];
+          gs.amap = st.amap;
+          gs.bmap = st.bmap;
+          gs.neg = st.neg;
+          gs.a_q = ijk[st.aq];
+          gs.a_p = ijk[st.ap];
+          gs.b_p = ijk[st.bp];
+          gs.ksteps = st.ksteps;
+        }
+        tiles += ((jt.M + GEMM_BM - 1) / GEMM_BM) * g.ntiles_n;
+        jobs.push_back(g);
+      }
+    }
+    CK(cudaMemcpyAsync(p->d_jobs, jobs.data(), jobs.size() * sizeof(GemmJob),
+                       cudaMemcpyHostToDevice, p->st));
+    CK(cudaMemcpyAsync(p->d_trip, trip.data(), trip.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, p->st));
+    CK(cudaMemcpyAsync(p->d_slot, slot.data(), slot.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, p->st));
+    CK(gemm_dmma_launch(c.maps, p->d_jobs, (int)jobs.size(), tiles, p->d_err,
+                        p->st));
+    EpiArgs e = c.epi;
+    e.ws = p->ws;
+    e.trip = p->d_trip;
+    e.partials = p->partials;
+    e.ntiles = c.ntiles;
+    e.tiles = c.d_tiles;
+    e.ctiles = c.ctiles;
+    if (c.type == 0)
+      CK(epi_aaa_launch(e, p->ft, (int)n, p->st));
+    else
+      CK(epi_aab_launch(e, p->ft, (int)n, p->st));
+    CK(reduce_partials_launch(p->partials, c.ntiles, (int)n, p->d_slot,
+                              p->e_slot, p->st));
+  }
+  return LIBPT_OK;
+}
+
+}  // namespace
+
+int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
+                const void *const *args, int dtype, int precision, bool host,
+                cudaStream_t st, libpt_plan **out) {
+  *out = nullptr;
+  if (kind < 0 || kind > 3 || dtype < 0 || dtype > 1 || !args) {
+    set_error("libpt_plan_create: bad kind/dtype/args");
+    return LIBPT_ERR_ARG;
+  }
+  if (precision != LIBPT_PREC_FP64) {
+    set_error("libpt_plan_create: unknown precision mode");
+    return LIBPT_ERR_ARG;
+  }
+  const bool unr = kind == 1 || kind == 3, ft = kind >= 2;
+  if (!unr) {
+    ob = oa;
+    vb = va;
+  }
+  const size_t lim = 1u << 15;
+  if (oa > lim || va > lim || ob > lim || vb > lim) {
+    set_error("libpt_plan_create: orbital space too large");
+    return LIBPT_ERR_ARG;
+  }
+  const int nargs = ft ? 10 : 7;
+  for (int a = 0; a < nargs; ++a)
+    if (!args[a]) {
+      set_error("libpt_plan_create: NULL tensor argument");
+      return LIBPT_ERR_ARG;
+    }
+  libpt_plan *p = new libpt_plan();
+  p->kind = kind;
+  p->unrestricted = unr;
+  p->ft = ft;
+  p->oa = (int)oa;
+  p->va = (int)va;
+  p->ob = (int)ob;
+  p->vb = (int)vb;
+  p->dtype = dtype;
+  p->precision = precision;
+  p->st = st;
+  p->factor = unr ? 1.0 : 2.0;   // src/pt.c:478, 534, 971, 1049
+  int r = LIBPT_OK;
+  do {
+    Sizes S{(int64_t)oa, (int64_t)va, (int64_t)ob, (int64_t)vb};
+    Uploader up{p, host, dtype == 1};
+    const int64_t nov = (int64_t)(oa * va + (unr ? ob * vb : 0));
+    if ((r = dalloc(p, (void **)&p->d_ov, nov * 8 + 8))) break;
+    if ((r = dalloc(p, (void **)&p->ov1, nov * 8 + 8))) break;
+    if ((r = dalloc(p, (void **)&p->ov2, nov * 8 + 8))) break;
+    // (T): d_ov f_ov t1 t2 i_oovo i_oovv i_ovvv
+    // (fT): d_ov f2_ov l1 t2 l2 i_oovv i2_t2f2_oovo i3_ovvv i6_oovo i7_ovvv
+    const void *a_d = args[0], *a_f = args[1], *a_1 = args[2];
+    const void *a_oovv = args[5];
+    if ((r = up.put(p->d_ov, a_d, 1, nov, nov))) break;
+    if ((r = up.put(p->ov1, a_1, 1, nov, nov))) break;
+    if ((r = up.put(p->ov2, a_f, 1, nov, nov))) break;
+    const int nb = unr ? 4 : 2;
+    const size_t es = dtype ? 4 : 8;
+    int64_t off = 0;
+    for (int b = 0; b < nb && !r; ++b) {
+      const int64_t n = S.oovv(b);
+      if ((r = dalloc(p, (void **)&p->oovv[b], n * 8 + 8))) break;
+      r = up.put(p->oovv[b], (const char *)a_oovv + off * es, 1, n, n);
+      off += n;
+    }
+    if (r) break;
+    if (!unr) p->oovv[3] = p->oovv[1];
+    if (!ft) {
+      r = upload_set(p, up, S, p->L, args[3], args[4], args[6]);
+    } else {
+      r = upload_set(p, up, S, p->L, args[4], args[8], args[9]);   // l2, i6, i7
+      if (!r) r = upload_set(p, up, S, p->R, args[3], args[6], args[7]);  // t2, i2, i3
+    }
+    if (r) break;
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+      set_error(std::string("preparing operands: ") +
+                cudaGetErrorString(cudaGetLastError()));
+      r = LIBPT_ERR_CUDA;
+      break;
+    }
+    if ((r = add_cases(p))) break;
+    if ((r = dalloc(p, (void **)&p->e_slot, (p->queue.size() + 1) * 8))) break;
+    if (cudaMemsetAsync(p->e_slot, 0, (p->queue.size() + 1) * 8, st) != cudaSuccess) {
+      r = LIBPT_ERR_CUDA;
+      break;
+    }
+    if ((r = dalloc(p, (void **)&p->d_err, sizeof(unsigned)))) break;
+    if (cudaMemsetAsync(p->d_err, 0, sizeof(unsigned), st) != cudaSuccess) {
+      r = LIBPT_ERR_CUDA;
+      break;
+    }
+    // workspace budget: half of what is free, between 64 MiB and 16 GiB;
+    // the buffer itself is allocated by the first batch that needs it
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    p->ws_budget = std::min<size_t>(std::max<size_t>(fr / 2, (size_t)64 << 20),
+                                    (size_t)16 << 30);
+  } while (0);
+  if (r) {
+    plan_destroy(p);
+    return r;
+  }
+  *out = p;
+  return LIBPT_OK;
+}
+
+void plan_destroy(libpt_plan *p) {
+  if (!p) return;
+  for (void *a : p->allocs) cudaFree(a);
+  delete p;
+}
+
+double plan_flops(const libpt_plan *p, int64_t first, int64_t n) {
+  double f = 0.0;
+  for (const SpinCase &c : p->cases) {
+    const int64_t lo = std::max(first, c.first);
+    const int64_t hi = std::min(first + n, c.first + c.count);
+    if (hi > lo) f += (double)(hi - lo) * c.flops_per_triple;
+  }
+  return f;
+}
+
+int plan_run(libpt_plan *p, const int64_t *idx, size_t n) {
+  const int64_t total = (int64_t)p->queue.size();
+  std::vector<std::vector<int64_t>> per(p->cases.size());
+  for (size_t x = 0; x < n; ++x) {
+    const int64_t q = idx ? idx[x] : (int64_t)x;
+    if (q < 0 || q >= total) {
+      set_error("libpt_plan_run: queue index out of range");
+      return LIBPT_ERR_ARG;
+    }
+    per[p->queue[q].x].push_back(q);
+  }
+  for (size_t ci = 0; ci < p->cases.size(); ++ci)
+    if (!per[ci].empty())
+      if (int r = run_case(p, p->cases[ci], per[ci])) return r;
+  return LIBPT_OK;
+}
+
+int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e) {
+  const size_t total = p->queue.size();
+  // the energy readback buffer comes from the caller's allocation hook
+  double *slots = static_cast<double *>(host_alloc((total + 1) * 8));
+  if (!slots) {
+    set_error("host allocation hook failed");
+    return LIBPT_ERR_NOMEM;
+  }
+  struct Guard {
+    double *q;
+    ~Guard() { host_free(q); }
+  } guard{slots};
+  CK(cudaMemcpyAsync(slots, p->e_slot, (total + 1) * 8,
+                     cudaMemcpyDeviceToHost, p->st));
+  unsigned err = 0;
+  CK(cudaMemcpyAsync(&err, p->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                     p->st));
+  CK(cudaStreamSynchronize(p->st));
+  if (err) {
+    set_error("a device-side wait exceeded its time limit");
+    return LIBPT_ERR_TIMEOUT;
+  }
+  // Neumaier-compensated sum in queue order
+  double s = 0.0, comp = 0.0;
+  const size_t m = idx ? n : total;
+  for (size_t x = 0; x < m; ++x) {
+    const int64_t q = idx ? idx[x] : (int64_t)x;
+    if (q < 0 || (size_t)q >= total) {
+      set_error("libpt_plan_energy: queue index out of range");
+      return LIBPT_ERR_ARG;
+    }
+    const double v = slots[q];
+    const double t = s + v;
+    comp += std::fabs(s) >= std::fabs(v) ? (s - t) + v : (v - t) + s;
+    s = t;
+  }
+  *e = p->factor * (s + comp);
+  return LIBPT_OK;
+}
+
+}  // namespace ptb

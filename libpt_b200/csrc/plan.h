@@ -1,0 +1,96 @@
+// Internal plan object behind the libpt_plan_* C API.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace ptb {
+
+void set_error(const std::string &msg);
+const char *last_error();
+// Host allocations through the libpt_set_malloc / libpt_set_free hooks.
+void *host_alloc(size_t n);
+void host_free(void *p);
+
+// Symbolic occupied index of a job segment: 0 = i, 1 = j, 2 = k.
+struct SegT {
+  int16_t amap, bmap, neg;
+  int8_t aq, ap, bp;
+  int32_t ksteps;
+};
+
+struct JobT {
+  int64_t off;      // output offset inside the triple's workspace slice
+  int32_t M, N;
+  int64_t ldc;
+  int nseg;
+  SegT seg[MAX_SEG];
+};
+
+// Padded device copies of one amplitude + integral set (index 0 aaaa,
+// 1 abab, 2 bbbb, 3 baba; packed pairs 0 aaaa, 1 bbbb).
+struct OperandSet {
+  double *tau[4] = {nullptr, nullptr, nullptr, nullptr};
+  double *taup[2] = {nullptr, nullptr};
+  double *ovvv[4] = {nullptr, nullptr, nullptr, nullptr};
+  double *oovo[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+struct SpinCase {
+  int type = 0;          // 0: same-spin (aaa), 1: mixed-spin (aab)
+  int flip = 0;          // aaa: 0 alpha, 1 beta; aab: 0 (a,a,b), 1 (b,b,a)
+  int oa = 0, va = 0, ob = 0, vb = 0;   // sizes as seen by this case
+  int64_t first = 0, count = 0;         // range in the triples queue
+  MapSet maps;
+  std::vector<JobT> jobs;               // per-triple job templates
+  EpiArgs epi;                          // fixed part of the epilogue args
+  int4 *d_tiles = nullptr;
+  int ntiles = 0, ctiles = 0;
+  double flops_per_triple = 0.0;        // reference GEMM flops
+};
+
+}  // namespace ptb
+
+struct libpt_plan {
+  int kind = 0;
+  bool unrestricted = false, ft = false;
+  int oa = 0, va = 0, ob = 0, vb = 0;
+  int dtype = 0, precision = 0;
+  cudaStream_t st = nullptr;
+  double factor = 1.0;
+  std::vector<void *> allocs;
+  ptb::OperandSet L, R;
+  double *d_ov = nullptr, *ov1 = nullptr, *ov2 = nullptr;
+  double *oovv[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<ptb::SpinCase> cases;
+  std::vector<int4> queue;              // (case, i, j, k)
+  double *e_slot = nullptr;
+  // batch resources
+  double *ws = nullptr;
+  size_t ws_bytes = 0;                  // current workspace allocation
+  size_t ws_budget = 0;                 // workspace size limit
+  double *partials = nullptr;
+  size_t partials_cap = 0;
+  ptb::GemmJob *d_jobs = nullptr;
+  size_t jobs_cap = 0;
+  int *d_trip = nullptr, *d_slot = nullptr;
+  size_t trip_cap = 0;
+  unsigned *d_err = nullptr;
+  size_t max_batch = 0;                 // 0: derive from the memory budget
+};
+
+namespace ptb {
+
+// args: pt.h tensors of `kind` in the reference's order; `host` selects host
+// (true) or device (false) pointers; dtype 0 = FP64, 1 = FP32.
+int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
+                const void *const *args, int dtype, int precision, bool host,
+                cudaStream_t st, libpt_plan **out);
+int plan_run(libpt_plan *p, const int64_t *idx, size_t n);
+int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e);
+void plan_destroy(libpt_plan *p);
+double plan_flops(const libpt_plan *p, int64_t first, int64_t n);
+
+}  // namespace ptb

@@ -1,0 +1,171 @@
+"""ctypes binding of libpt_b200.so (the C ABI declared in include/pt.h).
+
+The library must have been built (``python -m libpt_b200.build``); loading
+fails loudly otherwise -- there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpt_b200.so")
+
+PT_ARGS = ("d_ov", "f_ov", "t1", "t2", "i_oovo", "i_oovv", "i_ovvv")
+FT_ARGS = ("d_ov", "f2_ov", "l1", "t2", "l2", "i_oovv", "i2_t2f2_oovo",
+           "i3_ovvv", "i6_oovo", "i7_ovvv")
+KINDS = ("rpt", "upt", "rft", "uft")
+KIND_ID = {k: i for i, k in enumerate(KINDS)}
+
+LIBPT_OK = 0
+ERRORS = {1: "LIBPT_ERR_ARG", 2: "LIBPT_ERR_NOMEM", 3: "LIBPT_ERR_CUDA",
+          4: "LIBPT_ERR_TIMEOUT", 5: "LIBPT_ERR_UNSUPPORTED"}
+PREC_FP64 = 0
+
+_lib = None
+
+
+class LibptError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def args_of(kind):
+    return PT_ARGS if kind[1:] == "pt" else FT_ARGS
+
+
+def lib():
+    """The loaded library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run "
+                          "`python -m libpt_b200.build` (needs nvcc)")
+    L = ctypes.CDLL(LIB_PATH)
+    sz, dp, fp, vp = (ctypes.c_size_t, ctypes.POINTER(ctypes.c_double),
+                      ctypes.POINTER(ctypes.c_float), ctypes.c_void_p)
+    for kind in KINDS:
+        nsz = 2 if kind[0] == "r" else 4
+        npt = len(args_of(kind))
+        for mp, ptr in ((False, dp), (True, fp)):
+            name = "libpt_" + kind + ("_mp" if mp else "")
+            f = getattr(L, name)
+            f.restype = ctypes.c_double
+            f.argtypes = [sz] * nsz + [ptr] * npt
+            g = getattr(L, name + "_dev")
+            g.restype = ctypes.c_int
+            g.argtypes = [sz] * nsz + [vp] * npt + [vp, dp]
+    L.libpt_print_banner.restype = None
+    L.libpt_set_malloc.argtypes = [vp]
+    L.libpt_set_free.argtypes = [vp]
+    L.libpt_last_error.restype = ctypes.c_char_p
+    L.libpt_plan_create.restype = ctypes.c_int
+    L.libpt_plan_create.argtypes = [ctypes.c_int, sz, sz, sz, sz,
+                                    ctypes.POINTER(vp), ctypes.c_int,
+                                    ctypes.c_int, vp, ctypes.POINTER(vp)]
+    L.libpt_plan_queue_length.restype = ctypes.c_int64
+    L.libpt_plan_queue_length.argtypes = [vp]
+    L.libpt_plan_flops.restype = ctypes.c_double
+    L.libpt_plan_flops.argtypes = [vp, ctypes.c_int64, ctypes.c_int64]
+    L.libpt_plan_run.restype = ctypes.c_int
+    L.libpt_plan_run.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), sz]
+    L.libpt_plan_run_all.restype = ctypes.c_int
+    L.libpt_plan_run_all.argtypes = [vp]
+    L.libpt_plan_energy.restype = ctypes.c_int
+    L.libpt_plan_energy.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), sz,
+                                    dp]
+    L.libpt_plan_destroy.restype = ctypes.c_int
+    L.libpt_plan_destroy.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def check(code):
+    if code != LIBPT_OK:
+        raise LibptError(code, lib().libpt_last_error().decode())
+
+
+def _sizes(case):
+    s = [int(case["oa"]), int(case["va"])]
+    if case["kind"][0] == "u":
+        s += [int(case["ob"]), int(case["vb"])]
+    return s
+
+
+def solve_host(case, mp=False):
+    """Energy through the reference-compatible host-pointer entry point
+    (libpt_rpt / _upt / _rft / _uft and their _mp forms)."""
+    kind = case["kind"]
+    dt = np.float32 if mp else np.float64
+    ct = ctypes.c_float if mp else ctypes.c_double
+    arrs = [np.ascontiguousarray(case[n], dtype=dt) for n in args_of(kind)]
+    f = getattr(lib(), "libpt_" + kind + ("_mp" if mp else ""))
+    return f(*_sizes(case), *[a.ctypes.data_as(ctypes.POINTER(ct))
+                              for a in arrs])
+
+
+def solve_device(case, tensors, mp=False, stream=None):
+    """Energy through the device-pointer twin; `tensors` maps argument names
+    to CUDA torch tensors (contiguous, float64 or float32 for mp)."""
+    kind = case["kind"]
+    f = getattr(lib(), "libpt_" + kind + ("_mp" if mp else "") + "_dev")
+    e = ctypes.c_double(0.0)
+    ptrs = [ctypes.c_void_p(tensors[n].data_ptr()) for n in args_of(kind)]
+    check(f(*_sizes(case), *ptrs, ctypes.c_void_p(stream or 0),
+            ctypes.byref(e)))
+    return e.value
+
+
+class Plan:
+    """Resident operands of one solve and its triples queue (libpt_plan_*)."""
+
+    def __init__(self, case, tensors, mp=False, precision=PREC_FP64,
+                 stream=None):
+        kind = case["kind"]
+        s = _sizes(case)
+        if len(s) == 2:
+            s += s
+        ptrs = (ctypes.c_void_p * len(args_of(kind)))(
+            *[tensors[n].data_ptr() for n in args_of(kind)])
+        h = ctypes.c_void_p()
+        check(lib().libpt_plan_create(KIND_ID[kind], *s, ptrs, 1 if mp else 0,
+                                      precision, ctypes.c_void_p(stream or 0),
+                                      ctypes.byref(h)))
+        self.h = h
+        self.n = lib().libpt_plan_queue_length(h)
+
+    def flops(self, first=0, n=None):
+        return lib().libpt_plan_flops(self.h, first,
+                                      self.n - first if n is None else n)
+
+    def run(self, idx=None):
+        if idx is None:
+            check(lib().libpt_plan_run_all(self.h))
+            return
+        a = np.ascontiguousarray(idx, dtype=np.int64)
+        check(lib().libpt_plan_run(
+            self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), a.size))
+
+    def energy(self, idx=None):
+        e = ctypes.c_double(0.0)
+        if idx is None:
+            check(lib().libpt_plan_energy(self.h, None, 0, ctypes.byref(e)))
+        else:
+            a = np.ascontiguousarray(idx, dtype=np.int64)
+            check(lib().libpt_plan_energy(
+                self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                a.size, ctypes.byref(e)))
+        return e.value
+
+    def close(self):
+        if self.h:
+            lib().libpt_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,143 @@
+"""GPU parity: the device library against the reference's golden vectors and
+against the oracle (the reference build oracle/_ref when present, else our C
+restatement) on the same seeded inputs.
+
+Tolerances:
+  golden fixtures, FP64 and FP32 entry points: |dE| <= 1e-8 Eh (test.cpp:29)
+  FP64 vs the reference's own FP64 value:      |dE| <= 1e-9 Eh and
+                                               |dE| <= 1e-12 |E|
+  FP32 (*_mp) entry points vs the reference's *_mp: |dE| <= 1e-5 |E|
+"""
+import os
+
+import numpy as np
+import pytest
+
+from libpt_b200 import ffi, synth
+from oracle import oracle
+from tests.golden import fixtures
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN_EPS = 1e-8
+ABS64, REL64 = 1e-9, 1e-12
+
+
+def checker():
+    if os.path.exists(oracle.reference_path()):
+        return oracle.reference()
+    return oracle.restatement()
+
+
+@pytest.fixture(scope="module")
+def energies():
+    return fixtures.energies()
+
+
+def close64(e, ref):
+    return abs(e - ref) <= ABS64 and abs(e - ref) <= REL64 * abs(ref) + 1e-15
+
+
+def to_dev(case, mp=False):
+    import torch
+    dt = torch.float32 if mp else torch.float64
+    return {n: torch.as_tensor(np.ascontiguousarray(case[n])).to(
+        device="cuda", dtype=dt) for n in ffi.args_of(case["kind"])}
+
+
+@pytest.mark.parametrize("name", fixtures.NAMES)
+def test_golden_fp64(name, energies):
+    case = fixtures.load(name)
+    e = ffi.solve_host(case)
+    assert abs(e - case["e_ref"]) <= GOLDEN_EPS
+    assert close64(e, energies[name]["ref_fp64"])
+
+
+@pytest.mark.parametrize("name", fixtures.NAMES)
+def test_golden_mp(name, energies):
+    case = fixtures.load(name)
+    e = ffi.solve_host(case, mp=True)
+    assert abs(e - case["e_ref"]) <= GOLDEN_EPS
+    assert abs(e - energies[name]["ref_fp32"]) <= 1e-5 * abs(case["e_ref"])
+
+
+SYNTH = [
+    ("rpt", (5, 13)), ("rpt", (6, 20)), ("rpt", (8, 64)), ("rpt", (3, 2)),
+    ("rpt", (1, 6)), ("rpt", (2, 7)), ("rpt", (7, 33)), ("rpt", (4, 130)),
+    ("rpt", (20, 17)),
+    ("upt", (4, 11, 3, 13)), ("upt", (2, 3, 5, 8)), ("upt", (1, 5, 2, 6)),
+    ("upt", (6, 29, 5, 31)),
+    ("rft", (4, 10)), ("rft", (6, 37)),
+    ("uft", (3, 9, 4, 7)), ("uft", (2, 5, 1, 4)), ("uft", (5, 21, 4, 18)),
+]
+
+
+@pytest.mark.parametrize("kind,sz", SYNTH)
+def test_synthetic_fp64_vs_oracle(kind, sz):
+    case = synth.make(kind, *sz, seed=21, fock=1e-3)
+    ref = oracle.solve(checker(), case)
+    e = ffi.solve_host(case)
+    assert close64(e, ref), (e, ref, e - ref)
+
+
+@pytest.mark.parametrize("kind,sz", [("rpt", (5, 13)), ("upt", (4, 11, 3, 13)),
+                                     ("rft", (4, 10)), ("uft", (3, 9, 4, 7))])
+def test_synthetic_mp_vs_oracle(kind, sz):
+    case = synth.make(kind, *sz, seed=22, fock=1e-3)
+    ref = oracle.solve(checker(), case, mp=True)
+    e = ffi.solve_host(case, mp=True)
+    assert abs(e - ref) <= 1e-5 * abs(ref) + 1e-12
+
+
+@pytest.mark.parametrize("kind,sz", [("rpt", (5, 13)), ("upt", (4, 11, 3, 13)),
+                                     ("rft", (4, 10)), ("uft", (3, 9, 4, 7))])
+def test_device_twin_equals_host_entry(kind, sz):
+    case = synth.make(kind, *sz, seed=23, fock=1e-3)
+    e_host = ffi.solve_host(case)
+    e_dev = ffi.solve_device(case, to_dev(case))
+    assert e_dev == e_host          # same engine, same order: bitwise
+    e_mp = ffi.solve_device(case, to_dev(case, mp=True), mp=True)
+    assert e_mp == ffi.solve_host(case, mp=True)
+
+
+def test_zero_sizes():
+    for kind, sz in [("rpt", (0, 5)), ("rpt", (3, 0)), ("rpt", (3, 1)),
+                     ("upt", (2, 3, 0, 4)), ("uft", (0, 3, 2, 4))]:
+        case = synth.make(kind, *sz, seed=1)
+        assert ffi.solve_host(case) == oracle.solve(oracle.restatement(), case)
+
+
+def test_plan_pieces_equal_whole_and_are_deterministic():
+    case = synth.make("upt", 5, 17, 4, 19, seed=5, fock=1e-3)
+    t = to_dev(case)
+    p = ffi.Plan(case, t)
+    p.run()
+    e_all = p.energy()
+    q = ffi.Plan(case, t)
+    order = np.random.default_rng(0).permutation(q.n)
+    for chunk in np.array_split(order, 7):
+        q.run(chunk)
+    assert q.energy() == e_all
+    assert close64(e_all, oracle.solve(checker(), case))
+    # subset energies: sum over disjoint halves equals the whole
+    half = np.arange(q.n // 2)
+    rest = np.arange(q.n // 2, q.n)
+    assert q.energy(half) + q.energy(rest) == pytest.approx(e_all, rel=1e-14)
+    p.close()
+    q.close()
+
+
+def test_per_triple_energies_match_oracle():
+    case = synth.rpt_case(6, 21, seed=9, fock=1e-3)
+    p = ffi.Plan(case, to_dev(case))
+    p.run()
+    ref = np.concatenate([oracle.rpt_partials(case, 0),
+                          oracle.rpt_partials(case, 1)])
+    assert p.n == ref.size
+    got = np.array([p.energy([q]) for q in range(p.n)]) / 2.0
+    np.testing.assert_allclose(got, ref, rtol=1e-11, atol=1e-16)
+
+
+def test_repeat_is_bitwise_identical():
+    case = synth.make("rft", 5, 23, seed=31, fock=1e-3)
+    assert ffi.solve_host(case) == ffi.solve_host(case)
