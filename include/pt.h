@@ -174,11 +174,23 @@ int libpt_plan_run(libpt_plan *plan, const int64_t *idx, size_t n);
 /* Compute every queue entry (the whole solve).  Asynchronous. */
 int libpt_plan_run_all(libpt_plan *plan);
 /* Wait for the plan's stream and return the fixed-order, compensated sum of
- * the stored energies of entries idx[0..n) (idx == NULL: all entries),
- * scaled by the restricted factor when the whole queue is summed. */
+ * the stored energies of entries idx[0..n) (idx == NULL: all entries), each
+ * scaled by the restricted factor 2 (src/pt.c:478) for restricted kinds, so
+ * that the sum over the whole queue is the solver's result. */
 int libpt_plan_energy(libpt_plan *plan, const int64_t *idx, size_t n,
     double *e_out);
 int libpt_plan_destroy(libpt_plan *plan);
+
+/* Kernel timing for benchmarks: with timing enabled, each batch records CUDA
+ * events around its contraction (GEMM) and energy (epilogue) launches on the
+ * plan's stream.  libpt_plan_kernel_stats waits for the stream, returns the
+ * summed GEMM time (ms), the number of GEMM launches, their algorithmic flops,
+ * the summed epilogue time (ms) and the number of kernels launched by runs
+ * since the last call, and resets the counters.  Any pointer may be NULL. */
+int libpt_plan_timing(libpt_plan *plan, int enable);
+int libpt_plan_kernel_stats(libpt_plan *plan, double *gemm_ms,
+    int64_t *gemm_launches, double *gemm_flops, double *epi_ms,
+    int64_t *launches);
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -292,6 +292,27 @@ LIBPT_API int libpt_plan_energy(libpt_plan *plan, const int64_t *idx,
   return ptb::plan_energy(plan, idx, n, e_out);
 }
 
+LIBPT_API int libpt_plan_timing(libpt_plan *plan, int enable) {
+  if (!plan) {
+    ptb::set_error("libpt_plan_timing: NULL plan");
+    return LIBPT_ERR_ARG;
+  }
+  plan->timing = enable != 0;
+  return LIBPT_OK;
+}
+
+LIBPT_API int libpt_plan_kernel_stats(libpt_plan *plan, double *gemm_ms,
+                                      int64_t *gemm_launches,
+                                      double *gemm_flops, double *epi_ms,
+                                      int64_t *launches) {
+  if (!plan) {
+    ptb::set_error("libpt_plan_kernel_stats: NULL plan");
+    return LIBPT_ERR_ARG;
+  }
+  return ptb::plan_kernel_stats(plan, gemm_ms, gemm_launches, gemm_flops,
+                                epi_ms, launches);
+}
+
 LIBPT_API int libpt_plan_destroy(libpt_plan *plan) {
   ptb::plan_destroy(plan);
   return LIBPT_OK;

@@ -589,8 +589,18 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
                        cudaMemcpyHostToDevice, p->st));
     CK(cudaMemcpyAsync(p->d_slot, slot.data(), slot.size() * sizeof(int),
                        cudaMemcpyHostToDevice, p->st));
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (p->timing) {
+      for (int x = 0; x < 4; ++x) CK(cudaEventCreate(&ev[x]));
+      CK(cudaEventRecord(ev[0], p->st));
+    }
     CK(gemm_dmma_launch(c.maps, p->d_jobs, (int)jobs.size(), tiles, p->d_err,
                         p->st));
+    if (p->timing) {
+      CK(cudaEventRecord(ev[1], p->st));
+      CK(cudaEventRecord(ev[2], p->st));
+    }
+    p->launches += (tiles > 0) + (c.ntiles > 0) + 1;
     EpiArgs e = c.epi;
     e.ws = p->ws;
     e.trip = p->d_trip;
@@ -602,6 +612,16 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
       CK(epi_aaa_launch(e, p->ft, (int)n, p->st));
     else
       CK(epi_aab_launch(e, p->ft, (int)n, p->st));
+    if (p->timing) {
+      CK(cudaEventRecord(ev[3], p->st));
+      p->ev_gemm.push_back(ev[0]);
+      p->ev_gemm.push_back(ev[1]);
+      p->ev_epi.push_back(ev[2]);
+      p->ev_epi.push_back(ev[3]);
+      double fl = 0.0;
+      for (size_t t = 0; t < n; ++t) fl += c.flops_per_triple;
+      p->flops_gemm.push_back(fl);
+    }
     CK(reduce_partials_launch(p->partials, c.ntiles, (int)n, p->d_slot,
                               p->e_slot, p->st));
   }
@@ -715,8 +735,36 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
   return LIBPT_OK;
 }
 
+int plan_kernel_stats(libpt_plan *p, double *gemm_ms, int64_t *gemm_launches,
+                      double *gemm_flops, double *epi_ms, int64_t *launches) {
+  CK(cudaStreamSynchronize(p->st));
+  double g = 0.0, e = 0.0, f = 0.0;
+  for (size_t x = 0; x + 1 < p->ev_gemm.size(); x += 2) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, p->ev_gemm[x], p->ev_gemm[x + 1]));
+    g += ms;
+    CK(cudaEventElapsedTime(&ms, p->ev_epi[x], p->ev_epi[x + 1]));
+    e += ms;
+  }
+  for (double v : p->flops_gemm) f += v;
+  if (gemm_ms) *gemm_ms = g;
+  if (gemm_launches) *gemm_launches = (int64_t)(p->ev_gemm.size() / 2);
+  if (gemm_flops) *gemm_flops = f;
+  if (epi_ms) *epi_ms = e;
+  if (launches) *launches = p->launches;
+  for (cudaEvent_t ev : p->ev_gemm) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : p->ev_epi) cudaEventDestroy(ev);
+  p->ev_gemm.clear();
+  p->ev_epi.clear();
+  p->flops_gemm.clear();
+  p->launches = 0;
+  return LIBPT_OK;
+}
+
 void plan_destroy(libpt_plan *p) {
   if (!p) return;
+  for (cudaEvent_t ev : p->ev_gemm) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : p->ev_epi) cudaEventDestroy(ev);
   for (void *a : p->allocs) cudaFree(a);
   delete p;
 }

@@ -79,6 +79,11 @@ struct libpt_plan {
   size_t trip_cap = 0;
   unsigned *d_err = nullptr;
   size_t max_batch = 0;                 // 0: derive from the memory budget
+  // kernel timing (libpt_plan_timing): events around each launch
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_gemm, ev_epi;  // start/stop pairs
+  std::vector<double> flops_gemm;            // algorithmic flops per launch
+  int64_t launches = 0;                      // kernels launched by runs
 };
 
 namespace ptb {
@@ -92,5 +97,7 @@ int plan_run(libpt_plan *p, const int64_t *idx, size_t n);
 int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e);
 void plan_destroy(libpt_plan *p);
 double plan_flops(const libpt_plan *p, int64_t first, int64_t n);
+int plan_kernel_stats(libpt_plan *p, double *gemm_ms, int64_t *gemm_launches,
+                      double *gemm_flops, double *epi_ms, int64_t *launches);
 
 }  // namespace ptb

@@ -76,6 +76,13 @@ def lib():
     L.libpt_plan_energy.restype = ctypes.c_int
     L.libpt_plan_energy.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), sz,
                                     dp]
+    L.libpt_plan_timing.restype = ctypes.c_int
+    L.libpt_plan_timing.argtypes = [vp, ctypes.c_int]
+    L.libpt_plan_kernel_stats.restype = ctypes.c_int
+    L.libpt_plan_kernel_stats.argtypes = [
+        vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64),
+        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+        ctypes.POINTER(ctypes.c_int64)]
     L.libpt_plan_destroy.restype = ctypes.c_int
     L.libpt_plan_destroy.argtypes = [vp]
     _lib = L
@@ -158,6 +165,20 @@ class Plan:
                 self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
                 a.size, ctypes.byref(e)))
         return e.value
+
+    def timing(self, enable=True):
+        check(lib().libpt_plan_timing(self.h, 1 if enable else 0))
+
+    def kernel_stats(self):
+        """dict(gemm_ms, gemm_launches, gemm_flops, epi_ms, launches) since
+        the last call (kernel-level CUDA-event timings)."""
+        gm, gf, em = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        gl, la = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().libpt_plan_kernel_stats(self.h, ctypes.byref(gm),
+                                            ctypes.byref(gl), ctypes.byref(gf),
+                                            ctypes.byref(em), ctypes.byref(la)))
+        return dict(gemm_ms=gm.value, gemm_launches=gl.value,
+                    gemm_flops=gf.value, epi_ms=em.value, launches=la.value)
 
     def close(self):
         if self.h:

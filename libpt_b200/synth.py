@@ -165,6 +165,60 @@ def make(kind, oa, va, ob=None, vb=None, seed=0, fock=0.0):
     raise ValueError(kind)
 
 
+def rpt_case_device(o, v, seed=0, device="cuda", fock=0.0):
+    """Restricted (T) inputs generated on the GPU with torch, block by block,
+    for shapes too large for host generation (o=45, v=477 holds 74 GB).
+    Same distributions and symmetries as rpt_case (not the same numbers).
+    Returns (meta, tensors) with pt.h-layout float64 CUDA tensors."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    f64 = dict(dtype=torch.float64, device=device)
+
+    def normal(shape, std):
+        return torch.randn(shape, generator=g, **f64).mul_(std)
+
+    def oovv_like(std):
+        n = o * o * v * v
+        out = torch.empty(2 * n, **f64)
+        x = normal((o, o, v, v), std)
+        ab = out[n:].view(o, o, v, v)
+        torch.add(x, x.permute(1, 0, 3, 2), out=ab).mul_(0.5)
+        del x
+        torch.sub(ab, ab.transpose(2, 3), out=out[:n].view(o, o, v, v))
+        return out
+
+    n_o = o * o * v * o
+    i_oovo = torch.empty(2 * n_o, **f64)
+    ab = i_oovo[n_o:].view(o, o, v, o)
+    ab.copy_(normal((o, o, v, o), 5e-2))
+    torch.sub(ab, ab.transpose(0, 1), out=i_oovo[:n_o].view(o, o, v, o))
+
+    npr = v * (v - 1) // 2
+    n_aa = o * v * npr
+    i_ovvv = torch.empty(n_aa + o * v * v * v, **f64)
+    abv = i_ovvv[n_aa:].view(o, v, v, v)
+    rows, cols = torch.tril_indices(v, v, -1, device=device)
+    flat = rows * v + cols
+    aav = i_ovvv[:n_aa].view(o, v, npr)
+    for k in range(o):   # one k slice at a time keeps temporaries small
+        s = abv[k]
+        s.copy_(normal((v, v, v), 5e-2))
+        d = (s - s.transpose(1, 2)).reshape(v, v * v)
+        aav[k].copy_(d.index_select(1, flat))
+        del d
+    e_i = torch.rand(o, generator=g, **f64) * 1.2 - 1.5
+    e_a = torch.rand(v, generator=g, **f64) * 2.9 + 0.1
+    tensors = dict(
+        d_ov=(e_i[:, None] - e_a[None, :]).reshape(-1).contiguous(),
+        f_ov=(normal((o * v,), fock) if fock else torch.zeros(o * v, **f64)),
+        t1=normal((o * v,), 1e-3),
+        t2=oovv_like(1e-2), i_oovo=i_oovo, i_oovv=oovv_like(5e-2),
+        i_ovvv=i_ovvv)
+    meta = dict(kind="rpt", oa=o, va=v, ob=o, vb=v)
+    return meta, tensors
+
+
 def restricted_as_unrestricted(case):
     """A restricted case rewritten as the equivalent unrestricted input
     (bbbb = aaaa, baba = abab blocks), whose energy equals the restricted
