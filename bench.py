@@ -6,7 +6,7 @@
 
 One step = one pass of the triples engine over a fixed, evenly strided sample
 of the workload's triples queue (every 211th of its 58,740 triples: 68
-same-spin + 212 mixed-spin triples, ~1.1e14 flops), with every operand
+same-spin + 211 mixed-spin triples, ~1.1e14 flops), with every operand
 resident in HBM (74 GB of pt.h inputs; the engine's padded copies).  The
 metric is TFLOP/s of the reference's own contraction flops (twice the
 multiply-adds of its dgemm_ calls for those triples); the projected full-solve
