@@ -142,6 +142,28 @@ int libpt_uft_mp_dev(size_t oa, size_t va, size_t ob, size_t vb,
     const float *i3_ovvv, const float *i6_oovo, const float *i7_ovvv,
     void *stream, double *e_out);
 
+/* ---- allocation-free restricted (T) for small systems ------------------
+ * No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory: programs that give all device memory to their own
+ * pool allocator up front (a library cudaMalloc would fail or break their
+ * accounting) and latency-sensitive loops where cudaMalloc/cudaFree would
+ * synchronize the device.  Same arguments and result as libpt_rpt_dev (FP64
+ * device tensors in pt.h layout on the current device), but it allocates
+ * nothing: all scratch lives in one static device array of
+ * LIBPT_STATIC_SCRATCH_BYTES, which every GPU that loads the library keeps
+ * until the process exits.  Systems whose scratch does not fit are rejected
+ * with LIBPT_ERR_ARG before any work is queued (o = 8, v = 64 fits).
+ * The first call on a device looks up the array's device address (a one-time
+ * set-up per device); make that first call before any stream capture.
+ * Every call shares the array: calls whose work overlaps on the GPU race and
+ * give wrong results -- serialize them. */
+#define LIBPT_STATIC_SCRATCH_BYTES (64ull << 20)
+
+int libpt_rpt_dev_static(size_t oa, size_t va, const double *d_ov,
+    const double *f_ov, const double *t1, const double *t2,
+    const double *i_oovo, const double *i_oovv, const double *i_ovvv,
+    void *stream, double *e_out);
+
 /* ---- plans: resident operands, the triples queue run in pieces ----------
  *
  * A plan holds one solve's operands on the device in the library's padded

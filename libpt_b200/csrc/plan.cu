@@ -123,6 +123,17 @@ int map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld, int64_t K,
 int dalloc(libpt_plan *p, void **ptr, size_t bytes) {
   *ptr = nullptr;
   if (bytes == 0) bytes = 256;
+  if (p->arena) {   // carve from the caller's arena; never freed
+    const size_t off = (p->arena_used + 255) & ~size_t(255);
+    if (off + bytes > p->arena_size) {
+      set_error("scratch arena exhausted (" + std::to_string(off + bytes) +
+                " of " + std::to_string(p->arena_size) + " bytes)");
+      return LIBPT_ERR_NOMEM;
+    }
+    *ptr = p->arena + off;
+    p->arena_used = off + bytes;
+    return LIBPT_OK;
+  }
   cudaError_t e = cudaMalloc(ptr, bytes);
   if (e != cudaSuccess) {
     set_error("cudaMalloc(" + std::to_string(bytes) +
@@ -632,7 +643,8 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
 
 int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
                 const void *const *args, int dtype, int precision, bool host,
-                cudaStream_t st, libpt_plan **out) {
+                cudaStream_t st, libpt_plan **out, void *arena,
+                size_t arena_size) {
   *out = nullptr;
   if (kind < 0 || kind > 3 || dtype < 0 || dtype > 1 || !args) {
     set_error("libpt_plan_create: bad kind/dtype/args");
@@ -670,6 +682,8 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
   p->precision = precision;
   p->st = st;
   p->factor = unr ? 1.0 : 2.0;   // src/pt.c:478, 534, 971, 1049
+  p->arena = static_cast<char *>(arena);
+  p->arena_size = arena ? arena_size : 0;
   int r = LIBPT_OK;
   do {
     Sizes S{(int64_t)oa, (int64_t)va, (int64_t)ob, (int64_t)vb};
@@ -720,6 +734,41 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       r = LIBPT_ERR_CUDA;
       break;
     }
+    if (p->arena) {
+      // arena: size the batch buffers once, from what the arena has left
+      int64_t stride = 0, ntl = 0;
+      size_t njt = 0;
+      for (const SpinCase &c : p->cases)
+        if (c.count) {
+          stride = std::max<int64_t>(stride, c.epi.ws_stride);
+          ntl = std::max<int64_t>(ntl, c.ntiles);
+          njt = std::max(njt, c.jobs.size());
+        }
+      if (p->queue.empty()) break;
+      const size_t per = (size_t)stride * 8 + (size_t)ntl * 8 +
+                         njt * sizeof(GemmJob) + 16;
+      const size_t used = (p->arena_used + 255) & ~size_t(255);
+      const size_t left =
+          p->arena_size > used + 5 * 256 ? p->arena_size - used - 5 * 256 : 0;
+      const size_t nb = std::min<size_t>({left / per, (size_t)4096,
+                                          p->queue.size()});
+      if (nb == 0) {
+        set_error("scratch arena too small for one triple");
+        r = LIBPT_ERR_NOMEM;
+        break;
+      }
+      if ((r = dalloc(p, (void **)&p->ws, nb * stride * 8))) break;
+      if ((r = dalloc(p, (void **)&p->partials, nb * ntl * 8))) break;
+      if ((r = dalloc(p, (void **)&p->d_jobs, nb * njt * sizeof(GemmJob)))) break;
+      if ((r = dalloc(p, (void **)&p->d_trip, 3 * nb * sizeof(int)))) break;
+      if ((r = dalloc(p, (void **)&p->d_slot, nb * sizeof(int)))) break;
+      p->ws_bytes = p->ws_budget = nb * stride * 8;
+      p->partials_cap = nb * ntl;
+      p->jobs_cap = nb * njt;
+      p->trip_cap = nb;
+      p->max_batch = nb;
+      break;
+    }
     // workspace budget: half of what is free, between 64 MiB and 16 GiB;
     // the buffer itself is allocated by the first batch that needs it
     size_t fr = 0, tot = 0;
@@ -759,6 +808,28 @@ int plan_kernel_stats(libpt_plan *p, double *gemm_ms, int64_t *gemm_launches,
   p->flops_gemm.clear();
   p->launches = 0;
   return LIBPT_OK;
+}
+
+size_t rpt_arena_bytes(int64_t o, int64_t v, int64_t nb) {
+  auto r = [](int64_t b) {
+    return (size_t)((std::max<int64_t>(b, 1) + 255) & ~int64_t(255));
+  };
+  const int64_t np = npair(v);
+  size_t s = 3 * r(o * v * 8 + 8) + 2 * r(o * o * v * v * 8 + 8);
+  s += 2 * r(o * o * v * pad4(v) * 8) + 2 * r(o * o * v * pad4(o) * 8) +
+       r(o * v * pad4(np) * 8) + r(o * v * v * pad4(v) * 8) +
+       r(o * o * pad4(np) * 8);
+  const int64_t nbk = (v + EPI_A - 1) / EPI_A, ncb = (v + EPI_C - 1) / EPI_C;
+  const int64_t ntl = nbk * nbk * ncb;        // bound on tiles of a case
+  s += r(ntl * 16) + r(nbk * nbk * 16);       // tile tables
+  const int64_t nq = o * (o - 1) * (o - 2) / 6 + o * (o - 1) / 2 * o;
+  s += r((nq + 1) * 8) + r(4);
+  const int64_t st_aaa = pad32(v * pad4(np));
+  const int64_t st_aab = 2 * pad32(v * v * pad4(v)) + pad32(v * pad4(np));
+  const int64_t stride = std::max(st_aaa, st_aab);
+  s += r(nb * stride * 8) + r(nb * ntl * 8) +
+       r(nb * 3 * (int64_t)sizeof(GemmJob)) + r(nb * 12) + r(nb * 4);
+  return s;
 }
 
 void plan_destroy(libpt_plan *p) {

@@ -79,6 +79,10 @@ struct libpt_plan {
   size_t trip_cap = 0;
   unsigned *d_err = nullptr;
   size_t max_batch = 0;                 // 0: derive from the memory budget
+  // caller-provided device arena: when set, every device buffer of the plan
+  // is carved from it and nothing is allocated or freed
+  char *arena = nullptr;
+  size_t arena_size = 0, arena_used = 0;
   // kernel timing (libpt_plan_timing): events around each launch
   bool timing = false;
   std::vector<cudaEvent_t> ev_gemm, ev_epi;  // start/stop pairs
@@ -92,7 +96,11 @@ namespace ptb {
 // (true) or device (false) pointers; dtype 0 = FP64, 1 = FP32.
 int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
                 const void *const *args, int dtype, int precision, bool host,
-                cudaStream_t st, libpt_plan **out);
+                cudaStream_t st, libpt_plan **out, void *arena = nullptr,
+                size_t arena_size = 0);
+// Device bytes a restricted (T) plan of (o, v) takes from an arena when its
+// batches hold up to nb triples (arena mode, device sources).
+size_t rpt_arena_bytes(int64_t o, int64_t v, int64_t nb);
 int plan_run(libpt_plan *p, const int64_t *idx, size_t n);
 int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e);
 void plan_destroy(libpt_plan *p);
