@@ -15,7 +15,7 @@ namespace ptb {
 // OVVV/amplitude block (TMA view: dims (N, K, P)).  The slices are selected
 // by the occupied indices (Q, P) resp. (P) of the triple.
 
-constexpr int GEMM_BM = 128;   // rows of a CTA tile
+constexpr int GEMM_BM = 128;   // rows of a CTA tile (96 or 128, per case)
 constexpr int GEMM_BN = 128;   // columns of a CTA tile
 constexpr int GEMM_BK = 16;    // contraction depth of one pipeline stage
 constexpr int GEMM_STAGES = 5;
@@ -38,7 +38,8 @@ struct GemmJob {
   int32_t M, N;         // N <= ldc, N % 4 == 0
   int32_t ntiles_n;     // ceil(N / GEMM_BN)
   int32_t tile_begin;   // first flat tile index of this job in the launch
-  int32_t nseg, pad_;
+  int32_t nseg;
+  int32_t mtiles;       // ceil(M / BM); tiles are numbered M-tile fastest
   GemmSeg seg[MAX_SEG];
 };
 
@@ -46,16 +47,17 @@ struct MapSet {
   CUtensorMap m[MAX_MAPS];
 };
 
-size_t gemm_smem_bytes();
+size_t gemm_smem_bytes(int bm);
+// bm: CTA tile rows, 96 or 128 (the A views' box height must match).
 cudaError_t gemm_dmma_launch(const MapSet &maps, const GemmJob *d_jobs,
-                             int njobs, int total_tiles, unsigned *d_err,
-                             cudaStream_t st);
+                             int njobs, int total_tiles, int bm,
+                             unsigned *d_err, cudaStream_t st);
 
 // ---- energy epilogues ------------------------------------------------------
 
 constexpr int EPI_A = 8, EPI_B = 8, EPI_C = 32;   // tile extents a x b x c
 constexpr int EPI_THREADS = 256;
-constexpr int EPI_PAD = EPI_B + 1;                // smem row pad (banks)
+constexpr int EPI_CS = EPI_C + 2;                 // smem row stride (banks)
 
 // Arguments shared by the same-spin (aaa) and mixed-spin (aab) epilogues.
 struct EpiArgs {

@@ -13,7 +13,9 @@
 //
 // A CTA handles an 8 (a) x 8 (b) x 32 (c) tile of one triple; lanes run over
 // c so the loads of U1/T rows are coalesced, and the operands that are
-// contiguous in a or b (T[c][ab], U2, P) are staged through shared memory.
+// contiguous in a or b (T[c][ab], U2, P) are staged through shared memory
+// as [x][y][c] rows of EPI_CS = 34 doubles: the fill (8 consecutive y per
+// 8 lanes) and the reads (32 consecutive c) are both free of bank conflicts.
 // Each CTA writes one partial sum; reduce_partials adds them in a fixed order.
 #include "common.cuh"
 #include "engine.h"
@@ -59,13 +61,19 @@ __device__ __forceinline__ double disc_aaa(const double *ov, const double *g,
          ov[k * v + c] * gji[ba];
 }
 
+// Thread layout of both epilogues: warp w handles a = a0 + w, lane l handles
+// c = c0 + l, and each thread walks the tile's 8 values of b.  All loads a
+// thread needs are issued before they are used (unrolled, branch-free with
+// clamped indices and a validity mask), so many requests are in flight.
+
 template <bool FT>
-__global__ void __launch_bounds__(EPI_THREADS)
+__global__ void __launch_bounds__(EPI_THREADS, 2)
     epi_aaa_kernel(const EpiArgs p) {
   extern __shared__ double sm[];
-  // s3[a_][c_][b_] = T[c][pair(a,b)]  (and the R copy for (fT))
+  constexpr int S = EPI_A * EPI_B * EPI_CS;
+  constexpr int NIT = EPI_A * EPI_C * EPI_B / EPI_THREADS;
+  // s3[a_][b_][c_] = T[c][pair(a,b)]  (the R copy follows for (fT))
   double *s3 = sm;
-  double *s3r = sm + EPI_A * EPI_C * EPI_PAD;
 
   const int4 tl = p.tiles[blockIdx.x];
   const int a0 = tl.x, b0 = tl.y, c0 = tl.z;
@@ -77,34 +85,90 @@ __global__ void __launch_bounds__(EPI_THREADS)
   const double *R = FT ? base + p.offR[0] : nullptr;
   const int64_t ld = p.ld[0];
 
-  for (int e = threadIdx.x; e < EPI_A * EPI_C * EPI_B; e += EPI_THREADS) {
-    const int a_ = e / (EPI_C * EPI_B), c_ = (e / EPI_B) % EPI_C,
-              b_ = e % EPI_B;
-    const int a = a0 + a_, b = b0 + b_, c = c0 + c_;
-    const bool ok = a < v && b < a && c < b;
-    const int64_t off = (int64_t)c * ld + pairidx(a, b);
-    s3[(a_ * EPI_C + c_) * EPI_PAD + b_] = ok ? T[off] : 0.0;
-    if (FT) s3r[(a_ * EPI_C + c_) * EPI_PAD + b_] = ok ? R[off] : 0.0;
+  {
+    double vt[NIT], vr[NIT];
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int e = threadIdx.x + it * EPI_THREADS;
+      const int a_ = e / (EPI_C * EPI_B), c_ = (e / EPI_B) % EPI_C,
+                b_ = e % EPI_B;
+      const int a = a0 + a_, b = b0 + b_, c = c0 + c_;
+      const bool ok = a < v && b < a && c < b;
+      const int64_t off = ok ? (int64_t)c * ld + pairidx(a, b) : 0;
+      vt[it] = ok ? T[off] : 0.0;
+      vr[it] = (FT && ok) ? R[off] : 0.0;
+    }
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int e = threadIdx.x + it * EPI_THREADS;
+      const int a_ = e / (EPI_C * EPI_B), c_ = (e / EPI_B) % EPI_C,
+                b_ = e % EPI_B;
+      s3[(a_ * EPI_B + b_) * EPI_CS + c_] = vt[it];
+      if (FT) s3[S + (a_ * EPI_B + b_) * EPI_CS + c_] = vr[it];
+    }
   }
   __syncthreads();
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = c0 + lane;
+  const int a_ = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int a = a0 + a_, c = c0 + lane;
+  const int ac = a < v ? a : v - 1;       // clamped indices for addressing
+  const int cc = c < v ? c : v - 1;
+  // disconnected term (src/pt.c:162-175): the parts that depend on (a, c)
+  const int64_t sl1 = (int64_t)v * p.g1_ld_aa, sl2 = (int64_t)v * p.g2_ld_aa;
+  const double *g1jk = p.g1_aa + ((int64_t)j * o + k) * sl1;
+  const double *g1ik = p.g1_aa + ((int64_t)i * o + k) * sl1;
+  const double *g1ji = p.g1_aa + ((int64_t)j * o + i) * sl1;
+  const double *g2jk = p.g2_aa + ((int64_t)j * o + k) * sl2;
+  const double *g2ik = p.g2_aa + ((int64_t)i * o + k) * sl2;
+  const double *g2ji = p.g2_aa + ((int64_t)j * o + i) * sl2;
+  const double *u1 = p.ov1_a, *u2 = p.ov2_a;
+  const int64_t ac1 = (int64_t)ac * p.g1_ld_aa + cc,
+                ac2 = (int64_t)ac * p.g2_ld_aa + cc;
+  const double A1jk = g1jk[ac1], A1ik = g1ik[ac1], A1ji = g1ji[ac1];
+  const double A2jk = g2jk[ac2], A2ik = g2ik[ac2], A2ji = g2ji[ac2];
+  const double t1ia = u1[i * v + ac], t1ja = u1[j * v + ac],
+               t1ka = u1[k * v + ac];
+  const double t1ic = u1[i * v + cc], t1jc = u1[j * v + cc],
+               t1kc = u1[k * v + cc];
+  const double f_ia = u2[i * v + ac], f_ja = u2[j * v + ac],
+               f_ka = u2[k * v + ac];
+  const double f_ic = u2[i * v + cc], f_jc = u2[j * v + cc],
+               f_kc = u2[k * v + cc];
+  const double dia = p.d_a[i * v + ac], dkc = p.d_a[k * v + cc];
+
+  double w_[EPI_B], r_[EPI_B], x_[EPI_B], d_[EPI_B];
+  bool ok_[EPI_B];
+#pragma unroll
+  for (int b_ = 0; b_ < EPI_B; ++b_) {
+    const int b = b0 + b_;
+    ok_[b_] = a < v && b < a && c < b;
+    const int bc = b < v ? b : v - 1;
+    const int cb = ok_[b_] ? c : 0;          // pair index needs c < b
+    const int64_t t1 = (int64_t)ac * ld + pairidx(bc, cb);
+    const int64_t t2 = (int64_t)bc * ld + pairidx(ac, cb);
+    const int is = (a_ * EPI_B + b_) * EPI_CS + lane;
+    w_[b_] = T[t1] - T[t2] + s3[is];
+    r_[b_] = FT ? R[t1] - R[t2] + s3[S + is] : 0.0;
+    const int64_t bc1 = (int64_t)bc * p.g1_ld_aa + cc,
+                  bc2 = (int64_t)bc * p.g2_ld_aa + cc;
+    const int64_t ba1 = (int64_t)bc * p.g1_ld_aa + ac,
+                  ba2 = (int64_t)bc * p.g2_ld_aa + ac;
+    // the 9-term sums of src/pt.c:166-174 for (t1, i_oovv) and (f_ov, t2)
+    x_[b_] = t1ia * g1jk[bc1] - t1ja * g1ik[bc1] - t1ka * g1ji[bc1] -
+             u1[i * v + bc] * A1jk + u1[j * v + bc] * A1ik +
+             u1[k * v + bc] * A1ji - t1ic * g1jk[ba1] + t1jc * g1ik[ba1] +
+             t1kc * g1ji[ba1] +
+             f_ia * g2jk[bc2] - f_ja * g2ik[bc2] - f_ka * g2ji[bc2] -
+             u2[i * v + bc] * A2jk + u2[j * v + bc] * A2ik +
+             u2[k * v + bc] * A2ji - f_ic * g2jk[ba2] + f_jc * g2ik[ba2] +
+             f_kc * g2ji[ba2];
+    d_[b_] = (dia + p.d_a[j * v + bc]) + dkc;
+  }
   double e = 0.0;
-  for (int pr = warp; pr < EPI_A * EPI_B; pr += EPI_THREADS / 32) {
-    const int a_ = pr / EPI_B, b_ = pr % EPI_B;
-    const int a = a0 + a_, b = b0 + b_;
-    if (!(a < v && b < a && c < b)) continue;
-    const int64_t t1 = (int64_t)a * ld + pairidx(b, c);
-    const int64_t t2 = (int64_t)b * ld + pairidx(a, c);
-    const double w = T[t1] - T[t2] + s3[(a_ * EPI_C + lane) * EPI_PAD + b_];
-    const double r =
-        FT ? R[t1] - R[t2] + s3r[(a_ * EPI_C + lane) * EPI_PAD + b_] : w;
-    const double x =
-        disc_aaa(p.ov1_a, p.g1_aa, p.g1_ld_aa, o, v, i, j, k, a, b, c) +
-        disc_aaa(p.ov2_a, p.g2_aa, p.g2_ld_aa, o, v, i, j, k, a, b, c);
-    const double dn = p.d_a[i * v + a] + p.d_a[j * v + b] + p.d_a[k * v + c];
-    e += (w - x) * r / dn;
+#pragma unroll
+  for (int b_ = 0; b_ < EPI_B; ++b_) {
+    const double r = FT ? r_[b_] : w_[b_];
+    if (ok_[b_]) e += (w_[b_] - x_[b_]) * r / d_[b_];
   }
   const double s = block_sum(e);
   if (threadIdx.x == 0) p.partials[(int64_t)t * p.ntiles + blockIdx.x] = s;
@@ -113,12 +177,13 @@ __global__ void __launch_bounds__(EPI_THREADS)
 // ---------------------------------------------------------------- aab ----
 
 template <bool FT>
-__global__ void __launch_bounds__(EPI_THREADS)
+__global__ void __launch_bounds__(EPI_THREADS, 2)
     epi_aab_kernel(const EpiArgs p) {
   extern __shared__ double sm[];
-  constexpr int S = EPI_A * EPI_C * EPI_PAD;
-  // sx[a_][c_][b_] = U2[a][c][b];  sy[b_][c_][a_] = U2[b][c][a];
-  // sp[c_][a_][b_] = P[c][pair(a,b)]   (R copies follow for (fT))
+  constexpr int S = EPI_A * EPI_B * EPI_CS;
+  constexpr int NIT = EPI_A * EPI_C * EPI_B / EPI_THREADS;
+  // sx[a_][b_][c_] = U2[a][c][b];  sy[b_][a_][c_] = U2[b][c][a];
+  // sp[a_][b_][c_] = P[c][pair(a,b)]   (R copies follow for (fT))
   double *sx = sm, *sy = sm + S, *sp = sm + 2 * S;
 
   const int4 tl = p.tiles[blockIdx.x];
@@ -135,37 +200,39 @@ __global__ void __launch_bounds__(EPI_THREADS)
     const int64_t *off = side ? p.offR : p.offL;
     const double *U2 = base + off[1];
     const double *P = base + off[2];
-    double *x_ = sx + side * 3 * S, *y_ = sy + side * 3 * S,
-           *q_ = sp + side * 3 * S;
-    for (int e = threadIdx.x; e < EPI_A * EPI_C * EPI_B; e += EPI_THREADS) {
+    double vx[NIT], vy[NIT], vp[NIT];
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int e = threadIdx.x + it * EPI_THREADS;
       const int u = e / (EPI_C * EPI_B), c_ = (e / EPI_B) % EPI_C,
                 w = e % EPI_B;
       const int c = c0 + c_;
       const bool cok = c < vb;
-      {  // x_[u=a_][c_][w=b_] = U2[a][c][b]
-        const int a = a0 + u, b = b0 + w;
-        x_[(u * EPI_C + c_) * EPI_PAD + w] =
-            (cok && a < va && b < va) ? U2[(int64_t)a * ld2 + c * r2 + b]
-                                      : 0.0;
-      }
-      {  // y_[u=b_][c_][w=a_] = U2[b][c][a]
-        const int b = b0 + u, a = a0 + w;
-        y_[(u * EPI_C + c_) * EPI_PAD + w] =
-            (cok && a < va && b < va) ? U2[(int64_t)b * ld2 + c * r2 + a]
-                                      : 0.0;
-      }
-      {  // q_[c_][u=a_][w=b_] = P[c][pair(a,b)]
-        const int a = a0 + u, b = b0 + w;
-        q_[(c_ * EPI_A + u) * EPI_PAD + w] =
-            (cok && a < va && b < a) ? P[(int64_t)c * ldp + pairidx(a, b)]
-                                     : 0.0;
-      }
+      const int ax = a0 + u, bx = b0 + w;     // x: U2[a][c][b]
+      vx[it] = (cok && ax < va && bx < va)
+                   ? U2[(int64_t)ax * ld2 + c * r2 + bx] : 0.0;
+      const int by = b0 + u, ay = a0 + w;     // y: U2[b][c][a]
+      vy[it] = (cok && ay < va && by < va)
+                   ? U2[(int64_t)by * ld2 + c * r2 + ay] : 0.0;
+      vp[it] = (cok && ax < va && bx < ax)    // p: P[c][pair(a,b)]
+                   ? P[(int64_t)c * ldp + pairidx(ax, bx)] : 0.0;
+    }
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int e = threadIdx.x + it * EPI_THREADS;
+      const int u = e / (EPI_C * EPI_B), c_ = (e / EPI_B) % EPI_C,
+                w = e % EPI_B;
+      const int idx = side * 3 * S + (u * EPI_B + w) * EPI_CS + c_;
+      sx[idx] = vx[it];
+      sy[idx] = vy[it];
+      sp[idx] = vp[it];
     }
   }
   __syncthreads();
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int c = c0 + lane;
+  const int a_ = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int a = a0 + a_, c = c0 + lane;
+  const int ac = a < va ? a : va - 1, cc = c < vb ? c : vb - 1;
   const double *U1 = base + p.offL[0];
   const double *U1r = FT ? base + p.offR[0] : nullptr;
   // disconnected-term slices (src/pt.c:433-442)
@@ -175,38 +242,46 @@ __global__ void __launch_bounds__(EPI_THREADS)
   const double *g2jk = p.g2_ab + ((int64_t)j * ob + k) * va * p.g2_ld_ab;
   const double *g2ik = p.g2_ab + ((int64_t)i * ob + k) * va * p.g2_ld_ab;
   const double *g2ji = p.g2_aa + ((int64_t)j * oa + i) * va * p.g2_ld_aa;
+  const double *u1 = p.ov1_a, *u2 = p.ov2_a;
+  const int64_t ac1 = (int64_t)ac * p.g1_ld_ab + cc,
+                ac2 = (int64_t)ac * p.g2_ld_ab + cc;
+  const double A1jk = g1jk[ac1], A1ik = g1ik[ac1];
+  const double A2jk = g2jk[ac2], A2ik = g2ik[ac2];
+  const double t1ia = u1[i * va + ac], t1ja = u1[j * va + ac];
+  const double f_ia = u2[i * va + ac], f_ja = u2[j * va + ac];
+  const double o1k = p.ov1_b[k * vb + cc], o2k = p.ov2_b[k * vb + cc];
+  const double dia = p.d_a[i * va + ac], dkc = p.d_b[k * vb + cc];
+
+  double w_[EPI_B], r_[EPI_B], x_[EPI_B], d_[EPI_B];
+  bool ok_[EPI_B];
+#pragma unroll
+  for (int b_ = 0; b_ < EPI_B; ++b_) {
+    const int b = b0 + b_;
+    ok_[b_] = a < va && b < a && c < vb;
+    const int bc = b < va ? b : va - 1;
+    const int64_t u_ab = (int64_t)ac * ld1 + bc * r1 + cc;
+    const int64_t u_ba = (int64_t)bc * ld1 + ac * r1 + cc;
+    const int ix = (a_ * EPI_B + b_) * EPI_CS + lane;
+    const int iy = (b_ * EPI_A + a_) * EPI_CS + lane;
+    w_[b_] = U1[u_ab] + sx[ix] - U1[u_ba] - sy[iy] + sp[ix];
+    r_[b_] = FT ? U1r[u_ab] + sx[3 * S + ix] - U1r[u_ba] - sy[3 * S + iy] +
+                      sp[3 * S + ix]
+                : 0.0;
+    const int64_t bc1 = (int64_t)bc * p.g1_ld_ab + cc,
+                  bc2 = (int64_t)bc * p.g2_ld_ab + cc;
+    x_[b_] = t1ia * g1jk[bc1] - u1[i * va + bc] * A1jk - t1ja * g1ik[bc1] +
+             u1[j * va + bc] * A1ik +
+             o1k * g1ji[(int64_t)bc * p.g1_ld_aa + ac] +
+             f_ia * g2jk[bc2] - u2[i * va + bc] * A2jk - f_ja * g2ik[bc2] +
+             u2[j * va + bc] * A2ik +
+             o2k * g2ji[(int64_t)bc * p.g2_ld_aa + ac];
+    d_[b_] = (dia + p.d_a[j * va + bc]) + dkc;
+  }
   double e = 0.0;
-  if (c < vb) {
-    const double dk = p.d_b[k * vb + c];
-    const double o1k = p.ov1_b[k * vb + c], o2k = p.ov2_b[k * vb + c];
-    for (int pr = warp; pr < EPI_A * EPI_B; pr += EPI_THREADS / 32) {
-      const int a_ = pr / EPI_B, b_ = pr % EPI_B;
-      const int a = a0 + a_, b = b0 + b_;
-      if (!(a < va && b < a)) continue;
-      const int64_t u_ab = (int64_t)a * ld1 + b * r1 + c;
-      const int64_t u_ba = (int64_t)b * ld1 + a * r1 + c;
-      const int ix = (a_ * EPI_C + lane) * EPI_PAD + b_;
-      const int iy = (b_ * EPI_C + lane) * EPI_PAD + a_;
-      const int iq = (lane * EPI_A + a_) * EPI_PAD + b_;
-      const double w = U1[u_ab] + sx[ix] - U1[u_ba] - sy[iy] + sp[iq];
-      const double r =
-          FT ? U1r[u_ab] + sx[3 * S + ix] - U1r[u_ba] - sy[3 * S + iy] +
-                   sp[3 * S + iq]
-             : w;
-      const int64_t bc1 = (int64_t)b * p.g1_ld_ab + c,
-                    ac1 = (int64_t)a * p.g1_ld_ab + c;
-      const int64_t bc2 = (int64_t)b * p.g2_ld_ab + c,
-                    ac2 = (int64_t)a * p.g2_ld_ab + c;
-      const double x =
-          p.ov1_a[i * va + a] * g1jk[bc1] - p.ov1_a[i * va + b] * g1jk[ac1] -
-          p.ov1_a[j * va + a] * g1ik[bc1] + p.ov1_a[j * va + b] * g1ik[ac1] +
-          o1k * g1ji[(int64_t)b * p.g1_ld_aa + a] +
-          p.ov2_a[i * va + a] * g2jk[bc2] - p.ov2_a[i * va + b] * g2jk[ac2] -
-          p.ov2_a[j * va + a] * g2ik[bc2] + p.ov2_a[j * va + b] * g2ik[ac2] +
-          o2k * g2ji[(int64_t)b * p.g2_ld_aa + a];
-      const double dn = p.d_a[i * va + a] + p.d_a[j * va + b] + dk;
-      e += (w - x) * r / dn;
-    }
+#pragma unroll
+  for (int b_ = 0; b_ < EPI_B; ++b_) {
+    const double r = FT ? r_[b_] : w_[b_];
+    if (ok_[b_]) e += (w_[b_] - x_[b_]) * r / d_[b_];
   }
   const double s = block_sum(e);
   if (threadIdx.x == 0)
@@ -241,7 +316,7 @@ cudaError_t set_smem(K kern, size_t bytes) {
 }  // namespace
 
 size_t epi_smem_bytes(bool aab, bool ft) {
-  const size_t s = (size_t)EPI_A * EPI_C * EPI_PAD * sizeof(double);
+  const size_t s = (size_t)EPI_A * EPI_B * EPI_CS * sizeof(double);
   return (aab ? 3 : 1) * (ft ? 2 : 1) * s;
 }
 

@@ -1,20 +1,25 @@
 // FP64 contraction kernel: signed multi-segment GEMM on DMMA tensor cores.
 //
 // Replaces the reference's per-triple dgemm_ calls (src/pt.c:40-160): one
-// CTA computes a 128 x 128 tile of one triple's contraction output, summing
+// CTA computes a BM x 128 tile of one triple's contraction output, summing
 // all of that output's amplitude x integral products (up to six, each with
 // its own sign) in one K loop, so the permuted contributions the reference
 // adds one GEMM at a time (e.g. src/pt.c:236-290) meet in the accumulator.
 //
 // Pipeline: warp 8 (one elected lane) stages A and B tiles with TMA into a
 // GEMM_STAGES-deep ring of shared-memory buffers guarded by mbarriers;
-// warps 0-7 run mma.sync.m16n8k4.f64 on 64 x 32 warp tiles.
+// warps 0-7 run mma.sync.m16n8k4.f64 on (BM/2) x 32 warp tiles.
+// BM is 96 or 128 rows; the host picks the one that pads M less (v = 477
+// fills 5 x 96 = 480 rows against 4 x 128 = 512).
 //
 // Shared-memory layouts (no swizzle; TMA boxes are 32 bytes wide):
-//   A stage [k/4][m][k%4]   -- four boxes of (4 k x 128 rows)
+//   A stage [k/4][m][k%4]   -- four boxes of (4 k x BM rows)
 //   B stage [n/4][k][n%4]   -- thirty-two boxes of (4 n x 16 k)
 // so the fragment loads of a half-warp read 16 consecutive doubles (no bank
 // conflicts) for both operands.
+//
+// Tiles are numbered M-tile fastest inside a job, so the CTAs that share one
+// B (OVVV) tile run at the same time and the tile is fetched from DRAM once.
 #include "common.cuh"
 #include "engine.h"
 
@@ -22,9 +27,13 @@ namespace ptb {
 
 namespace {
 
-constexpr int BM = GEMM_BM, BN = GEMM_BN, BK = GEMM_BK, ST = GEMM_STAGES;
+constexpr int BN = GEMM_BN, BK = GEMM_BK, ST = GEMM_STAGES;
 constexpr int NCW = GEMM_CONSUMER_WARPS;
-constexpr uint32_t STAGE_BYTES = (BM * BK + BK * BN) * sizeof(double);
+
+template <int BM>
+constexpr uint32_t stage_bytes() {
+  return (BM * BK + BK * BN) * sizeof(double);
+}
 
 __device__ __forceinline__ int find_job(const GemmJob *jobs, int njobs,
                                         int tile) {
@@ -39,10 +48,16 @@ __device__ __forceinline__ int find_job(const GemmJob *jobs, int njobs,
   return lo;
 }
 
+// One CTA of GEMM_THREADS (9 warps) per SM.  With 9 warps one SM
+// sub-partition hosts 3 of them, which bounds the kernel at 168 registers per
+// thread (16K registers per sub-partition); the 128-row tile's 64 FP64
+// accumulators per thread fit that without spilling.
+template <int BM>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     gemm_dmma_kernel(const __grid_constant__ MapSet maps,
                      const GemmJob *__restrict__ jobs, int njobs,
                      unsigned *err) {
+  constexpr int MF = BM / 32;   // m16 fragments per warp (2 warp rows)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double *sA = reinterpret_cast<double *>(smem_raw);
   double *sB = sA + ST * BM * BK;
@@ -52,8 +67,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
   const int tile = blockIdx.x;
   const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
   const int local = tile - job.tile_begin;
-  const int m0 = (local / job.ntiles_n) * BM;
-  const int n0 = (local % job.ntiles_n) * BN;
+  const int m0 = (local % job.mtiles) * BM;
+  const int n0 = (local / job.mtiles) * BN;
   const int nseg = job.nseg;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -82,7 +97,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             ok = false;
             break;
           }
-          mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+          mbar_arrive_expect_tx(&full[stage], stage_bytes<BM>());
           double *dA = sA + stage * BM * BK;
           double *dB = sB + stage * BK * BN;
           const int k0 = ks * BK;
@@ -112,22 +127,22 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
   }
 
   // ---------------- consumers ----------------
-  const int wm = (warp >> 2) * 64;   // warp tile origin in the CTA tile
+  const int wm = (warp >> 2) * (BM / 2);   // warp tile origin in the CTA tile
   const int wn = (warp & 3) * 32;
   const int g = lane >> 2, t = lane & 3;
 
-  double acc[4][4][4];
+  double acc[MF][4][4];
 #pragma unroll
-  for (int f = 0; f < 4; ++f)
+  for (int f = 0; f < MF; ++f)
 #pragma unroll
     for (int h = 0; h < 4; ++h)
 #pragma unroll
       for (int e = 0; e < 4; ++e) acc[f][h][e] = 0.0;
 
   // Per-lane fragment offsets inside one stage.
-  int aoff[4];
+  int aoff[MF];
 #pragma unroll
-  for (int f = 0; f < 4; ++f) aoff[f] = (wm + 16 * f + g) * 4 + t;
+  for (int f = 0; f < MF; ++f) aoff[f] = (wm + 16 * f + g) * 4 + t;
   int boff[4];
 #pragma unroll
   for (int h = 0; h < 4; ++h) {
@@ -151,16 +166,16 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       const double *B = sB + stage * BK * BN;
 #pragma unroll
       for (int kq = 0; kq < BK / 4; ++kq) {
-        double a0[4], a1[4], b[4];
+        double a0[MF], a1[MF], b[4];
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
+        for (int f = 0; f < MF; ++f) {
           a0[f] = flip_sign(A[kq * BM * 4 + aoff[f]], mask);
           a1[f] = flip_sign(A[kq * BM * 4 + aoff[f] + 32], mask);
         }
 #pragma unroll
         for (int h = 0; h < 4; ++h) b[h] = B[kq * 16 + boff[h]];
 #pragma unroll
-        for (int f = 0; f < 4; ++f)
+        for (int f = 0; f < MF; ++f)
 #pragma unroll
           for (int h = 0; h < 4; ++h) dmma_16x8x4(acc[f][h], a0[f], a1[f], b[h]);
       }
@@ -178,7 +193,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
   double *out = job.out;
   const int64_t ldc = job.ldc;
 #pragma unroll
-  for (int f = 0; f < 4; ++f) {
+  for (int f = 0; f < MF; ++f) {
     const int r = m0 + wm + 16 * f + g;
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
@@ -195,28 +210,37 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
   }
 }
 
-}  // namespace
-
-size_t gemm_smem_bytes() {
-  return (size_t)ST * STAGE_BYTES + 2 * ST * sizeof(uint64_t);
-}
-
-cudaError_t gemm_dmma_launch(const MapSet &maps, const GemmJob *d_jobs,
-                             int njobs, int total_tiles, unsigned *d_err,
-                             cudaStream_t st) {
-  if (total_tiles <= 0) return cudaSuccess;
+template <int BM>
+cudaError_t launch(const MapSet &maps, const GemmJob *d_jobs, int njobs,
+                   int total_tiles, unsigned *d_err, cudaStream_t st) {
   static bool configured = false;
-  const size_t smem = gemm_smem_bytes();
+  const size_t smem = gemm_smem_bytes(BM);
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(
-        gemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        gemm_dmma_kernel<BM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int)smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  gemm_dmma_kernel<<<total_tiles, GEMM_THREADS, smem, st>>>(maps, d_jobs,
-                                                            njobs, d_err);
+  gemm_dmma_kernel<BM><<<total_tiles, GEMM_THREADS, smem, st>>>(
+      maps, d_jobs, njobs, d_err);
   return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t gemm_smem_bytes(int bm) {
+  return (size_t)ST * (bm * BK + BK * BN) * sizeof(double) +
+         2 * ST * sizeof(uint64_t);
+}
+
+cudaError_t gemm_dmma_launch(const MapSet &maps, const GemmJob *d_jobs,
+                             int njobs, int total_tiles, int bm,
+                             unsigned *d_err, cudaStream_t st) {
+  if (total_tiles <= 0) return cudaSuccess;
+  if (bm == 96)
+    return launch<96>(maps, d_jobs, njobs, total_tiles, d_err, st);
+  return launch<128>(maps, d_jobs, njobs, total_tiles, d_err, st);
 }
 
 }  // namespace ptb

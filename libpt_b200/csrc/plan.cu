@@ -66,9 +66,9 @@ EncodeTiledFn encode_fn() {
 }
 
 // A-view of a padded block [P][Q][R][Kpad] with logical K: dims (K, R, Q, P),
-// box (4, GEMM_BM, 1, 1).
+// box (4, bm, 1, 1).
 int map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R, int64_t Q,
-          int64_t P) {
+          int64_t P, int bm) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -81,7 +81,7 @@ int map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R, int64_t Q,
                         (cuuint64_t)std::max<int64_t>(P, 1)};
   cuuint64_t strides[3] = {(cuuint64_t)(kp * 8), (cuuint64_t)(R * kp * 8),
                            (cuuint64_t)(Q * R * kp * 8)};
-  cuuint32_t box[4] = {4, (cuuint32_t)GEMM_BM, 1, 1};
+  cuuint32_t box[4] = {4, (cuuint32_t)bm, 1, 1};
   cuuint32_t es[4] = {1, 1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)p, dims,
                    strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -293,8 +293,8 @@ int build_aaa(libpt_plan *p, SpinCase &c) {
   for (int x = 0; x < nset; ++x) {
     const OperandSet &set = x ? p->R : p->L;
     const int b0 = 4 * x;
-    if (int r = map_a(&c.maps.m[b0 + 0], set.tau[s ? 2 : 0], v, v, o, o)) return r;
-    if (int r = map_a(&c.maps.m[b0 + 1], set.oovo[s ? 2 : 0], o, v, o, o)) return r;
+    if (int r = map_a(&c.maps.m[b0 + 0], set.tau[s ? 2 : 0], v, v, o, o, c.bm)) return r;
+    if (int r = map_a(&c.maps.m[b0 + 1], set.oovo[s ? 2 : 0], o, v, o, o, c.bm)) return r;
     if (int r = map_b(&c.maps.m[b0 + 2], set.ovvv[s ? 2 : 0], np, ldT, v, o)) return r;
     if (int r = map_b(&c.maps.m[b0 + 3], set.taup[s], np, ldT, o, o)) return r;
     JobT j;
@@ -379,12 +379,12 @@ int build_aab(libpt_plan *p, SpinCase &c) {
     const OperandSet &S = x ? p->R : p->L;
     CUtensorMap *m = &c.maps.m[12 * x];
     int r;
-    if ((r = map_a(&m[0], S.tau[Taa], va, va, oa, oa))) return r;
-    if ((r = map_a(&m[1], S.tau[Tab], vb, va, ob, oa))) return r;
-    if ((r = map_a(&m[2], S.tau[Tba], va, vb, oa, ob))) return r;
-    if ((r = map_a(&m[3], S.oovo[Taa], oa, va, oa, oa))) return r;
-    if ((r = map_a(&m[4], S.oovo[Tab], ob, va, ob, oa))) return r;
-    if ((r = map_a(&m[5], S.oovo[Tba], oa, vb, oa, ob))) return r;
+    if ((r = map_a(&m[0], S.tau[Taa], va, va, oa, oa, c.bm))) return r;
+    if ((r = map_a(&m[1], S.tau[Tab], vb, va, ob, oa, c.bm))) return r;
+    if ((r = map_a(&m[2], S.tau[Tba], va, vb, oa, ob, c.bm))) return r;
+    if ((r = map_a(&m[3], S.oovo[Taa], oa, va, oa, oa, c.bm))) return r;
+    if ((r = map_a(&m[4], S.oovo[Tab], ob, va, ob, oa, c.bm))) return r;
+    if ((r = map_a(&m[5], S.oovo[Tba], oa, vb, oa, ob, c.bm))) return r;
     if ((r = map_b(&m[6], S.ovvv[Taa], np, ldP, va, oa))) return r;
     if ((r = map_b(&m[7], S.ovvv[Tab], ld1, ld1, vb, oa))) return r;
     if ((r = map_b(&m[8], S.ovvv[Tba], ld2, ld2, va, ob))) return r;
@@ -517,6 +517,12 @@ int add_cases(libpt_plan *p) {
   if (p->unrestricted) add(1, 1, ob, vb, oa, va);
   for (SpinCase &c : p->cases) {
     if (c.count == 0) continue;
+    // CTA tile rows: the choice that pads the GEMM rows (va, and vb for the
+    // mixed-spin P job) least; ties go to 128 (more CTAs)
+    auto padded = [](int64_t m, int64_t bm) { return (m + bm - 1) / bm * bm; };
+    const int64_t w128 = padded(c.va, 128) + (c.type ? padded(c.vb, 128) : 0);
+    const int64_t w96 = padded(c.va, 96) + (c.type ? padded(c.vb, 96) : 0);
+    c.bm = w96 < w128 ? 96 : 128;
     int r = c.type == 0 ? build_aaa(p, c) : build_aab(p, c);
     if (r) return r;
   }
@@ -577,6 +583,7 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
         g.M = jt.M;
         g.N = jt.N;
         g.ntiles_n = (jt.N + GEMM_BN - 1) / GEMM_BN;
+        g.mtiles = (jt.M + c.bm - 1) / c.bm;
         g.tile_begin = tiles;
         g.nseg = jt.nseg;
         for (int s = 0; s < jt.nseg; ++s) {
@@ -590,7 +597,7 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
           gs.b_p = ijk[st.bp];
           gs.ksteps = st.ksteps;
         }
-        tiles += ((jt.M + GEMM_BM - 1) / GEMM_BM) * g.ntiles_n;
+        tiles += g.mtiles * g.ntiles_n;
         jobs.push_back(g);
       }
     }
@@ -605,8 +612,8 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
       for (int x = 0; x < 4; ++x) CK(cudaEventCreate(&ev[x]));
       CK(cudaEventRecord(ev[0], p->st));
     }
-    CK(gemm_dmma_launch(c.maps, p->d_jobs, (int)jobs.size(), tiles, p->d_err,
-                        p->st));
+    CK(gemm_dmma_launch(c.maps, p->d_jobs, (int)jobs.size(), tiles, c.bm,
+                        p->d_err, p->st));
     if (p->timing) {
       CK(cudaEventRecord(ev[1], p->st));
       CK(cudaEventRecord(ev[2], p->st));

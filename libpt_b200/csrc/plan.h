@@ -49,6 +49,7 @@ struct SpinCase {
   int4 *d_tiles = nullptr;
   int ntiles = 0, ctiles = 0;
   double flops_per_triple = 0.0;        // reference GEMM flops
+  int bm = GEMM_BM;                     // CTA tile rows of this case's GEMMs
 };
 
 }  // namespace ptb
