@@ -98,6 +98,18 @@ const char *libpt_last_error(void);
 /* ---- precision modes ---------------------------------------------------- */
 
 #define LIBPT_PREC_FP64   0   /* FP64 DMMA tensor-core contractions          */
+#define LIBPT_PREC_TF32X3 1   /* 3xTF32 on tcgen05 tensor cores (hi*hi +
+                                 hi*lo + lo*hi, FP32 accumulation in TMEM):
+                                 ~1e-5 relative per contraction element; the
+                                 *_mp entry points use it when the environment
+                                 sets LIBPT_MP_PRECISION=tf32x3 (otherwise
+                                 they evaluate FP32 inputs in FP64)          */
+
+/* Built-in self-test of a contraction kernel: C = A B1 - A B2 on random
+ * m x k and k x n operands, against an FP64 reference computed on the device;
+ * writes max|C - C_ref| / max|C_ref| to *rel_err.  precision selects the
+ * kernel (LIBPT_PREC_*).  No counterpart in the reference. */
+int libpt_selftest(int precision, int m, int n, int k, double *rel_err);
 
 /* ---- device-pointer twins ----------------------------------------------
  * Same arguments as the reference entry points, but every tensor is a

@@ -24,8 +24,8 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
          "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 HOST_CXX = "/usr/bin/g++"   # the image's $CXX wrapper lacks some runtime specs
 
-SOURCES = ["gemm_dmma.cu", "epilogue.cu", "prep.cu", "plan.cu", "api.cpp",
-           "noalloc.cu"]
+SOURCES = ["gemm_dmma.cu", "gemm_tc.cu", "epilogue.cu", "prep.cu", "plan.cu", "api.cpp",
+           "noalloc.cu", "selftest.cu"]
 HEADERS = ["common.cuh", "engine.h", "plan.h"]
 
 

@@ -53,6 +53,35 @@ cudaError_t gemm_dmma_launch(const MapSet &maps, const GemmJob *d_jobs,
                              int njobs, int total_tiles, int bm,
                              unsigned *d_err, cudaStream_t st);
 
+// ---- tensor-core (tcgen05) GEMM --------------------------------------------
+//
+// Operands as "planes" (e.g. TF32 hi / lo parts).  A planes: [P][Q][R][Kp]
+// (K contiguous) seen as (K, R, Q, P) with boxes (KCHUNK bytes, 128, 1, 1);
+// B planes transposed, [P][N][Kp], seen as (K, N, P) with boxes
+// (KCHUNK bytes, TC_BN, 1); both 128B-swizzled.  Plane p of an operand whose
+// first plane is map i is map i + p.
+
+constexpr int TC_BM = 128;    // rows of a tile (TMEM lanes)
+constexpr int TC_BN = 256;    // columns of a tile
+constexpr int TC_TF32 = 0;    // kinds
+constexpr int TC_INT8 = 1;
+constexpr int TC_MAX_MAPS = 48;
+
+struct TcMapSet {
+  CUtensorMap m[TC_MAX_MAPS];
+};
+
+struct TcProducts {           // acc[c] += A_plane[pa] * B_plane[pb]^T
+  int8_t pa[16], pb[16], acc[16];
+  int n;
+};
+
+int tc_kchunk_elems(int kind);   // K elements per pipeline stage
+cudaError_t gemm_tc_launch(int kind, const TcMapSet &maps,
+                           const GemmJob *d_jobs, int njobs, int total_tiles,
+                           const TcProducts &prods, unsigned *d_err,
+                           cudaStream_t st);
+
 // ---- energy epilogues ------------------------------------------------------
 
 constexpr int EPI_A = 8, EPI_B = 8, EPI_C = 32;   // tile extents a x b x c
@@ -103,5 +132,13 @@ cudaError_t repack_launch(const void *src, bool src_fp32, double *dst,
 cudaError_t pack_pairs_launch(const double *tau, double *out, int64_t npq,
                               int v, int64_t ldv, int64_t ldp,
                               cudaStream_t st);
+// TF32 hi/lo planes of n FP64 values (exact FP32 values).
+cudaError_t split_tf32_launch(const double *src, float *hi, float *lo,
+                              int64_t n, cudaStream_t st);
+// src[P][K][ldn] -> hi/lo[P][N][ldk] (transposed; k >= K zero-filled).
+cudaError_t transpose_split_tf32_launch(const double *src, float *hi,
+                                        float *lo, int64_t P, int K,
+                                        int64_t N, int64_t ldn, int64_t ldk,
+                                        cudaStream_t st);
 
 }  // namespace ptb

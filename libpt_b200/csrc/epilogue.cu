@@ -44,23 +44,6 @@ __device__ double block_sum(double x) {
 
 // ---------------------------------------------------------------- aaa ----
 
-// Disconnected term of a same-spin triple (src/pt.c:162-175).
-__device__ __forceinline__ double disc_aaa(const double *ov, const double *g,
-                                           int64_t gld, int o, int v, int i,
-                                           int j, int k, int a, int b, int c) {
-  const int64_t sl = (int64_t)v * gld;   // one [v][gld] slice of oovv
-  const double *gjk = g + ((int64_t)j * o + k) * sl;
-  const double *gik = g + ((int64_t)i * o + k) * sl;
-  const double *gji = g + ((int64_t)j * o + i) * sl;
-  const int64_t bc = (int64_t)b * gld + c, ac = (int64_t)a * gld + c,
-                ba = (int64_t)b * gld + a;
-  return ov[i * v + a] * gjk[bc] - ov[j * v + a] * gik[bc] -
-         ov[k * v + a] * gji[bc] - ov[i * v + b] * gjk[ac] +
-         ov[j * v + b] * gik[ac] + ov[k * v + b] * gji[ac] -
-         ov[i * v + c] * gjk[ba] + ov[j * v + c] * gik[ba] +
-         ov[k * v + c] * gji[ba];
-}
-
 // Thread layout of both epilogues: warp w handles a = a0 + w, lane l handles
 // c = c0 + l, and each thread walks the tile's 8 values of b.  All loads a
 // thread needs are issued before they are used (unrolled, branch-free with

@@ -1,0 +1,342 @@
+// Tensor-core (tcgen05) contraction kernel for the multi-segment jobs.
+//
+// Same job/segment structure as gemm_dmma.cu (one triple's contraction
+// output = sum of signed amplitude x integral products), but the products
+// run on the 5th-generation tensor cores with accumulators in TMEM.  Each
+// operand is stored as PA (A side) / PB (B side) "planes" -- e.g. the high
+// and low TF32 parts of an FP32 value -- and a tile's result is
+//     acc[c] = sum over the products (pa, pb, c) of A_plane[pa] * B_plane[pb]^T
+// combined by the epilogue into FP64.  3xTF32: planes {hi, lo}, products
+// hi*hi + hi*lo + lo*hi into one FP32 accumulator (the *_mp entry points).
+//
+// Warp roles (persistent CTA, one per SM):
+//   warp 0      TMA producer: A and B plane tiles of one 128-byte K chunk per
+//               pipeline stage (128B-swizzled, K-major)
+//   warp 1      TMEM owner and MMA issuer: one thread issues tcgen05.mma for
+//               every product and K step, tcgen05.commit frees the stage
+//   warps 2-5   epilogue: tcgen05.ld of the finished accumulator (double
+//               buffered in TMEM so the next tile's MMAs overlap), FP64 store
+// All mbarrier waits are bounded; on expiry the kernel records the error,
+// stops issuing, still releases TMEM, and returns.
+#include "common.cuh"
+#include "engine.h"
+
+namespace ptb {
+
+namespace {
+
+constexpr int BM = TC_BM;          // 128 rows (TMEM lanes)
+constexpr int KCHUNK = 128;        // bytes of K per stage (one swizzle row)
+
+__device__ __forceinline__ int find_job(const GemmJob *jobs, int njobs,
+                                        int tile) {
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (jobs[mid].tile_begin <= tile)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Shared-memory matrix descriptor, K-major operand in 128B-swizzled rows of
+// 128 bytes, 8-row core groups 1024 bytes apart (SBO), sm_100 version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) |
+         ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+template <int KIND>
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db,
+                                       uint32_t idesc, uint32_t accum) {
+  if (KIND == TC_TF32)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+            tmem),
+        "l"(da), "l"(db), "r"(idesc), "r"(accum));
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+            tmem),
+        "l"(da), "l"(db), "r"(idesc), "r"(accum));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+      "[%0];" ::"r"(smem_u32(bar))
+      : "memory");
+}
+
+// 32 lanes x 32 consecutive 32-bit columns of TMEM.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, "
+      "[%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]),
+        "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]),
+        "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+        "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+        "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+
+// Instruction descriptor: M = 128, N = BN, K-major A and B; TF32 inputs with
+// FP32 accumulation, or signed INT8 inputs with INT32 accumulation.
+template <int KIND, int BN>
+__host__ __device__ constexpr uint32_t tc_idesc() {
+  return (KIND == TC_TF32 ? ((1u << 4) | (2u << 7) | (2u << 10))
+                          : ((2u << 4) | (1u << 7) | (1u << 10))) |
+         ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+template <int KIND, int BN, int PA, int PB, int NACC, int ST>
+struct TcCfg {
+  static constexpr int A_TILE = BM * KCHUNK;      // bytes per A plane tile
+  static constexpr int B_TILE = BN * KCHUNK;      // bytes per B plane tile
+  static constexpr int STAGE = PA * A_TILE + PB * B_TILE;
+  static constexpr int KSTEP = 32;                // bytes of K per MMA
+  static constexpr int TMEM_COLS = 2 * NACC * BN; // double-buffered accumulators
+  static constexpr int SMEM = ST * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+  static_assert(TMEM_COLS <= 512, "TMEM holds 512 columns");
+};
+
+template <int KIND, int BN, int PA, int PB, int NACC, int ST>
+__global__ void __launch_bounds__(192, 1)
+    gemm_tc_kernel(const __grid_constant__ TcMapSet maps,
+                   const GemmJob *__restrict__ jobs, int njobs,
+                   int total_tiles, const __grid_constant__ TcProducts prods,
+                   unsigned *err) {
+  using C = TcCfg<KIND, BN, PA, PB, NACC, ST>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  unsigned char *smem = smem_raw + ((1024 - (raw & 1023)) & 1023);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + ST * C::STAGE);
+  uint64_t *empty = full + ST;
+  uint64_t *accfull = empty + ST;      // [2]
+  uint64_t *accempty = accfull + 2;    // [2]
+  uint32_t *taddr_s = reinterpret_cast<uint32_t *>(accempty + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ST; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accfull[b], 1);
+      mbar_init(&accempty[b], 128);
+    }
+    mbar_fence_init();
+  }
+  if (warp == 1) {
+    asm volatile(
+        "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::
+            "r"(smem_u32(taddr_s)),
+        "r"((uint32_t)C::TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *taddr_s;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- TMA producer ----------------
+    int stage = 0;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
+      const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
+      const int local = tile - job.tile_begin;
+      const int m0 = (local % job.mtiles) * BM;
+      const int n0 = (local / job.mtiles) * BN;
+      for (int s = 0; s < job.nseg && ok; ++s) {
+        const GemmSeg sg = job.seg[s];
+        for (int ks = 0; ks < sg.ksteps; ++ks) {
+          if (!mbar_wait(&empty[stage], phase ^ 1u, err)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&full[stage], C::STAGE);
+          unsigned char *st_base = smem + stage * C::STAGE;
+          const int k0 = ks * (KIND == TC_TF32 ? KCHUNK / 4 : KCHUNK);
+#pragma unroll
+          for (int p = 0; p < PA; ++p)
+            tma_load_4d(st_base + p * C::A_TILE, &maps.m[sg.amap + p],
+                        &full[stage], k0, m0, sg.a_q, sg.a_p);
+#pragma unroll
+          for (int p = 0; p < PB; ++p)
+            tma_load_3d(st_base + PA * C::A_TILE + p * C::B_TILE,
+                        &maps.m[sg.bmap + p], &full[stage], k0, n0, sg.b_p);
+          if (++stage == ST) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer ----------------
+    int stage = 0;
+    uint32_t phase = 0;
+    bool ok = true;
+    int it = 0;
+    for (int tile = blockIdx.x; tile < total_tiles && ok;
+         tile += gridDim.x, ++it) {
+      const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
+      const int ab = it & 1;
+      if (!mbar_wait(&accempty[ab], (uint32_t)(((it >> 1) & 1) ^ 1), err)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t acc0 = tmem + (uint32_t)(ab * NACC * BN);
+      uint32_t started = 0;   // bit c: accumulator c has been written
+      for (int s = 0; s < job.nseg && ok; ++s) {
+        const GemmSeg sg = job.seg[s];
+        const uint32_t neg = (KIND == TC_TF32 && sg.neg) ? (1u << 13) : 0u;
+        for (int ks = 0; ks < sg.ksteps; ++ks) {
+          if (!mbar_wait(&full[stage], phase, err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sa = smem_u32(smem + stage * C::STAGE);
+          const uint32_t sb = sa + PA * C::A_TILE;
+          for (int q = 0; q < prods.n; ++q) {
+            const int c = prods.acc[q];
+            const uint64_t da = sw128_desc(sa + prods.pa[q] * C::A_TILE);
+            const uint64_t db = sw128_desc(sb + prods.pb[q] * C::B_TILE);
+            const uint32_t tm = acc0 + (uint32_t)(c * BN);
+#pragma unroll
+            for (int kk = 0; kk < KCHUNK / C::KSTEP; ++kk) {
+              // advancing the start address by 32 B steps through the
+              // swizzled 128-byte row (K-major SW128 layout)
+              tc_mma<KIND>(tm, da + (uint64_t)(kk * C::KSTEP >> 4),
+                           db + (uint64_t)(kk * C::KSTEP >> 4),
+                           tc_idesc<KIND, BN>() | neg,
+                           (started >> c) & 1u);
+              started |= 1u << c;
+            }
+          }
+          tc_commit(&empty[stage]);   // stage reusable once these MMAs finish
+          if (++stage == ST) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      if (ok) tc_commit(&accfull[ab]);
+    }
+  } else if (warp >= 2) {
+    // ---------------- epilogue ----------------
+    const int q = warp & 3;            // TMEM lane quarter of this warp
+    int it = 0;
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++it) {
+      const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
+      const int local = tile - job.tile_begin;
+      const int m0 = (local % job.mtiles) * BM;
+      const int n0 = (local / job.mtiles) * BN;
+      const int ab = it & 1;
+      if (!mbar_wait(&accfull[ab], (uint32_t)((it >> 1) & 1), err)) break;
+      tc_fence_after();
+      const int row = m0 + 32 * q + lane;
+      double *orow = job.out + (int64_t)row * job.ldc;
+      const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) +
+                             (uint32_t)(ab * NACC * BN);
+#pragma unroll 1
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        uint32_t r[NACC][32];
+#pragma unroll
+        for (int a = 0; a < NACC; ++a) tmem_ld32(tbase + a * BN + c0, r[a]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < job.M) {
+#pragma unroll
+          for (int x = 0; x < 32; x += 2) {
+            const int col = n0 + c0 + x;
+            if (col < job.N) {
+              double v0, v1;
+              if (KIND == TC_TF32) {
+                v0 = (double)__uint_as_float(r[0][x]);
+                v1 = (double)__uint_as_float(r[0][x + 1]);
+              } else {
+                v0 = 0.0;
+                v1 = 0.0;
+#pragma unroll
+                for (int a = 0; a < NACC; ++a) {
+                  v0 += ldexp((double)(int)r[a][x], -7 * (a + 2));
+                  v1 += ldexp((double)(int)r[a][x + 1], -7 * (a + 2));
+                }
+              }
+              *reinterpret_cast<double2 *>(orow + col) = make_double2(v0, v1);
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&accempty[ab]);
+    }
+  }
+  // all roles done: release TMEM
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(
+                     tmem),
+                 "r"((uint32_t)C::TMEM_COLS));
+  }
+}
+
+template <int KIND, int BN, int PA, int PB, int NACC, int ST>
+cudaError_t launch(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
+                   int total_tiles, const TcProducts &prods, unsigned *d_err,
+                   cudaStream_t st) {
+  using C = TcCfg<KIND, BN, PA, PB, NACC, ST>;
+  static bool configured = false;
+  auto kern = gemm_tc_kernel<KIND, BN, PA, PB, NACC, ST>;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(
+        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  int grid = total_tiles < 148 ? total_tiles : 148;
+  kern<<<grid, 192, C::SMEM, st>>>(maps, d_jobs, njobs, total_tiles, prods,
+                                   d_err);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+int tc_kchunk_elems(int kind) { return kind == TC_TF32 ? KCHUNK / 4 : KCHUNK; }
+
+cudaError_t gemm_tc_launch(int kind, const TcMapSet &maps,
+                           const GemmJob *d_jobs, int njobs, int total_tiles,
+                           const TcProducts &prods, unsigned *d_err,
+                           cudaStream_t st) {
+  if (total_tiles <= 0) return cudaSuccess;
+  if (kind == TC_TF32)
+    return launch<TC_TF32, TC_BN, 2, 2, 1, 2>(maps, d_jobs, njobs, total_tiles,
+                                              prods, d_err, st);
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace ptb

@@ -120,6 +120,115 @@ int map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld, int64_t K,
   return LIBPT_OK;
 }
 
+int tc_encode(CUtensorMap *m, const float *p, int rank, const cuuint64_t *dims,
+              const cuuint64_t *strides, const cuuint32_t *box) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return LIBPT_ERR_CUDA;
+  }
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, (void *)p, dims,
+                   strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (tensor-core view) failed: " +
+              std::to_string(r));
+    return LIBPT_ERR_CUDA;
+  }
+  return LIBPT_OK;
+}
+
+int dalloc(libpt_plan *p, void **ptr, size_t bytes);
+
+}  // namespace
+
+int dmma_map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R,
+               int64_t Q, int64_t P, int bm) {
+  return map_a(m, p, K, R, Q, P, bm);
+}
+
+int dmma_map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld,
+               int64_t K, int64_t P) {
+  return map_b(m, p, N, Nld, K, P);
+}
+
+int tc_map_a(CUtensorMap *m, const float *p, int64_t K, int64_t R, int64_t Q,
+             int64_t P) {
+  const int64_t kp = pad4(K);
+  cuuint64_t dims[4] = {(cuuint64_t)std::max<int64_t>(K, 1),
+                        (cuuint64_t)std::max<int64_t>(R, 1),
+                        (cuuint64_t)std::max<int64_t>(Q, 1),
+                        (cuuint64_t)std::max<int64_t>(P, 1)};
+  cuuint64_t strides[3] = {(cuuint64_t)(kp * 4), (cuuint64_t)(R * kp * 4),
+                           (cuuint64_t)(Q * R * kp * 4)};
+  cuuint32_t box[4] = {(cuuint32_t)tc_kchunk_elems(TC_TF32), (cuuint32_t)TC_BM,
+                       1, 1};
+  return tc_encode(m, p, 4, dims, strides, box);
+}
+
+int tc_map_b(CUtensorMap *m, const float *p, int64_t K, int64_t N, int64_t P) {
+  const int64_t kp = pad4(K);
+  cuuint64_t dims[3] = {(cuuint64_t)std::max<int64_t>(K, 1),
+                        (cuuint64_t)std::max<int64_t>(N, 1),
+                        (cuuint64_t)std::max<int64_t>(P, 1)};
+  cuuint64_t strides[2] = {(cuuint64_t)(kp * 4), (cuuint64_t)(N * kp * 4)};
+  cuuint32_t box[3] = {(cuuint32_t)tc_kchunk_elems(TC_TF32), (cuuint32_t)TC_BN,
+                       1};
+  return tc_encode(m, p, 3, dims, strides, box);
+}
+
+namespace {
+
+// TF32 planes of an operand, made once per (source block, role).
+int get_planes(libpt_plan *p, const OpDesc &d, Planes *out) {
+  const std::pair<const double *, int> key(d.src, d.role);
+  for (auto &e : p->planes)
+    if (e.first == key) {
+      *out = e.second;
+      return LIBPT_OK;
+    }
+  Planes pl;
+  const int64_t kp = pad4(d.K);
+  if (d.role == 0) {
+    const int64_t n = d.P * d.Q * d.R * kp;
+    if (dalloc(p, (void **)&pl.hi, n * 4) || dalloc(p, (void **)&pl.lo, n * 4))
+      return LIBPT_ERR_NOMEM;
+    CK(split_tf32_launch(d.src, pl.hi, pl.lo, n, p->st));
+  } else {
+    const int64_t n = d.P * d.N * kp;
+    if (dalloc(p, (void **)&pl.hi, n * 4) || dalloc(p, (void **)&pl.lo, n * 4))
+      return LIBPT_ERR_NOMEM;
+    CK(transpose_split_tf32_launch(d.src, pl.hi, pl.lo, d.P, (int)d.K, d.N,
+                                   d.Nld, kp, p->st));
+  }
+  p->planes.push_back({key, pl});
+  *out = pl;
+  return LIBPT_OK;
+}
+
+// Tensor-core views of a case: plane pairs at map indices 2i, 2i+1.
+int build_tc(libpt_plan *p, SpinCase &c) {
+  for (int i = 0; i < MAX_MAPS; ++i) {
+    const OpDesc &d = c.opd[i];
+    if (d.role < 0) continue;
+    if (2 * i + 1 >= TC_MAX_MAPS) {
+      set_error("too many tensor-core operand views");
+      return LIBPT_ERR_ARG;
+    }
+    Planes pl;
+    if (int r = get_planes(p, d, &pl)) return r;
+    for (int h = 0; h < 2; ++h) {
+      const float *pp = h ? pl.lo : pl.hi;
+      int r = d.role == 0 ? tc_map_a(&c.tcmaps.m[2 * i + h], pp, d.K, d.R, d.Q, d.P)
+                          : tc_map_b(&c.tcmaps.m[2 * i + h], pp, d.K, d.N, d.P);
+      if (r) return r;
+    }
+  }
+  return LIBPT_OK;
+}
+
 int dalloc(libpt_plan *p, void **ptr, size_t bytes) {
   *ptr = nullptr;
   if (bytes == 0) bytes = 256;
@@ -274,10 +383,36 @@ SegT seg(int amap, int bmap, bool neg, int aq, int ap, int bp, int64_t k) {
   s.ap = (int8_t)ap;
   s.bp = (int8_t)bp;
   s.ksteps = ksteps(k);
+  s.k = (int32_t)k;
   return s;
 }
 
 enum { I = 0, J = 1, K = 2 };
+
+// Encode a DMMA view and remember what it views (for the tensor-core path).
+int reg_a(SpinCase &c, int idx, const double *ptr, int64_t Kd, int64_t R,
+          int64_t Q, int64_t P) {
+  OpDesc &d = c.opd[idx];
+  d.role = 0;
+  d.src = ptr;
+  d.K = Kd;
+  d.R = R;
+  d.Q = Q;
+  d.P = P;
+  return map_a(&c.maps.m[idx], ptr, Kd, R, Q, P, c.bm);
+}
+
+int reg_b(SpinCase &c, int idx, const double *ptr, int64_t N, int64_t Nld,
+          int64_t Kd, int64_t P) {
+  OpDesc &d = c.opd[idx];
+  d.role = 1;
+  d.src = ptr;
+  d.K = Kd;
+  d.N = N;
+  d.Nld = Nld;
+  d.P = P;
+  return map_b(&c.maps.m[idx], ptr, N, Nld, Kd, P);
+}
 
 // Same-spin case: four maps per operand set, one job (T) per set.
 int build_aaa(libpt_plan *p, SpinCase &c) {
@@ -293,10 +428,10 @@ int build_aaa(libpt_plan *p, SpinCase &c) {
   for (int x = 0; x < nset; ++x) {
     const OperandSet &set = x ? p->R : p->L;
     const int b0 = 4 * x;
-    if (int r = map_a(&c.maps.m[b0 + 0], set.tau[s ? 2 : 0], v, v, o, o, c.bm)) return r;
-    if (int r = map_a(&c.maps.m[b0 + 1], set.oovo[s ? 2 : 0], o, v, o, o, c.bm)) return r;
-    if (int r = map_b(&c.maps.m[b0 + 2], set.ovvv[s ? 2 : 0], np, ldT, v, o)) return r;
-    if (int r = map_b(&c.maps.m[b0 + 3], set.taup[s], np, ldT, o, o)) return r;
+    if (int r = reg_a(c, b0 + 0, set.tau[s ? 2 : 0], v, v, o, o)) return r;
+    if (int r = reg_a(c, b0 + 1, set.oovo[s ? 2 : 0], o, v, o, o)) return r;
+    if (int r = reg_b(c, b0 + 2, set.ovvv[s ? 2 : 0], np, ldT, v, o)) return r;
+    if (int r = reg_b(c, b0 + 3, set.taup[s], np, ldT, o, o)) return r;
     JobT j;
     j.off = offs[x];
     j.M = (int)v;
@@ -377,20 +512,20 @@ int build_aab(libpt_plan *p, SpinCase &c) {
   const int Taa = f ? 2 : 0, Tab = f ? 3 : 1, Tba = f ? 1 : 3;
   for (int x = 0; x < nset; ++x) {
     const OperandSet &S = x ? p->R : p->L;
-    CUtensorMap *m = &c.maps.m[12 * x];
+    const int m = 12 * x;
     int r;
-    if ((r = map_a(&m[0], S.tau[Taa], va, va, oa, oa, c.bm))) return r;
-    if ((r = map_a(&m[1], S.tau[Tab], vb, va, ob, oa, c.bm))) return r;
-    if ((r = map_a(&m[2], S.tau[Tba], va, vb, oa, ob, c.bm))) return r;
-    if ((r = map_a(&m[3], S.oovo[Taa], oa, va, oa, oa, c.bm))) return r;
-    if ((r = map_a(&m[4], S.oovo[Tab], ob, va, ob, oa, c.bm))) return r;
-    if ((r = map_a(&m[5], S.oovo[Tba], oa, vb, oa, ob, c.bm))) return r;
-    if ((r = map_b(&m[6], S.ovvv[Taa], np, ldP, va, oa))) return r;
-    if ((r = map_b(&m[7], S.ovvv[Tab], ld1, ld1, vb, oa))) return r;
-    if ((r = map_b(&m[8], S.ovvv[Tba], ld2, ld2, va, ob))) return r;
-    if ((r = map_b(&m[9], S.taup[f], np, ldP, oa, oa))) return r;
-    if ((r = map_b(&m[10], S.tau[Tab], ld1, ld1, ob, oa))) return r;
-    if ((r = map_b(&m[11], S.tau[Tba], ld2, ld2, oa, ob))) return r;
+    if ((r = reg_a(c, m + 0, S.tau[Taa], va, va, oa, oa))) return r;
+    if ((r = reg_a(c, m + 1, S.tau[Tab], vb, va, ob, oa))) return r;
+    if ((r = reg_a(c, m + 2, S.tau[Tba], va, vb, oa, ob))) return r;
+    if ((r = reg_a(c, m + 3, S.oovo[Taa], oa, va, oa, oa))) return r;
+    if ((r = reg_a(c, m + 4, S.oovo[Tab], ob, va, ob, oa))) return r;
+    if ((r = reg_a(c, m + 5, S.oovo[Tba], oa, vb, oa, ob))) return r;
+    if ((r = reg_b(c, m + 6, S.ovvv[Taa], np, ldP, va, oa))) return r;
+    if ((r = reg_b(c, m + 7, S.ovvv[Tab], ld1, ld1, vb, oa))) return r;
+    if ((r = reg_b(c, m + 8, S.ovvv[Tba], ld2, ld2, va, ob))) return r;
+    if ((r = reg_b(c, m + 9, S.taup[f], np, ldP, oa, oa))) return r;
+    if ((r = reg_b(c, m + 10, S.tau[Tab], ld1, ld1, ob, oa))) return r;
+    if ((r = reg_b(c, m + 11, S.tau[Tba], ld2, ld2, oa, ob))) return r;
     const int b = 12 * x;
     JobT u1, u2, pp;
     // U1[x][y,c] = -t_ik I_j + t_jk I_i + O_jk t_i - O_ik t_j
@@ -524,6 +659,7 @@ int add_cases(libpt_plan *p) {
     const int64_t w96 = padded(c.va, 96) + (c.type ? padded(c.vb, 96) : 0);
     c.bm = w96 < w128 ? 96 : 128;
     int r = c.type == 0 ? build_aaa(p, c) : build_aab(p, c);
+    if (!r && p->precision == LIBPT_PREC_TF32X3) r = build_tc(p, c);
     if (r) return r;
   }
   return LIBPT_OK;
@@ -582,20 +718,24 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
         g.ldc = jt.ldc;
         g.M = jt.M;
         g.N = jt.N;
-        g.ntiles_n = (jt.N + GEMM_BN - 1) / GEMM_BN;
-        g.mtiles = (jt.M + c.bm - 1) / c.bm;
+        const bool tc = p->precision == LIBPT_PREC_TF32X3;
+        const int bn = tc ? TC_BN : GEMM_BN, bmr = tc ? TC_BM : c.bm;
+        g.ntiles_n = (jt.N + bn - 1) / bn;
+        g.mtiles = (jt.M + bmr - 1) / bmr;
         g.tile_begin = tiles;
         g.nseg = jt.nseg;
         for (int s = 0; s < jt.nseg; ++s) {
           const SegT &st = jt.seg[s];
           GemmSeg &gs = g.seg[s];
-          gs.amap = st.amap;
-          gs.bmap = st.bmap;
+          gs.amap = (int16_t)(tc ? 2 * st.amap : st.amap);
+          gs.bmap = (int16_t)(tc ? 2 * st.bmap : st.bmap);
           gs.neg = st.neg;
           gs.a_q = ijk[st.aq];
           gs.a_p = ijk[st.ap];
           gs.b_p = ijk[st.bp];
-          gs.ksteps = st.ksteps;
+          gs.ksteps = tc ? (st.k + tc_kchunk_elems(TC_TF32) - 1) /
+                               tc_kchunk_elems(TC_TF32)
+                         : st.ksteps;
         }
         tiles += g.mtiles * g.ntiles_n;
         jobs.push_back(g);
@@ -612,8 +752,22 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
       for (int x = 0; x < 4; ++x) CK(cudaEventCreate(&ev[x]));
       CK(cudaEventRecord(ev[0], p->st));
     }
-    CK(gemm_dmma_launch(c.maps, p->d_jobs, (int)jobs.size(), tiles, c.bm,
-                        p->d_err, p->st));
+    if (p->precision == LIBPT_PREC_TF32X3) {
+      TcProducts pr;
+      memset(&pr, 0, sizeof(pr));
+      const int8_t pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};   // hh + hl + lh
+      for (int q = 0; q < 3; ++q) {
+        pr.pa[q] = pa[q];
+        pr.pb[q] = pb[q];
+        pr.acc[q] = 0;
+      }
+      pr.n = 3;
+      CK(gemm_tc_launch(TC_TF32, c.tcmaps, p->d_jobs, (int)jobs.size(), tiles,
+                        pr, p->d_err, p->st));
+    } else {
+      CK(gemm_dmma_launch(c.maps, p->d_jobs, (int)jobs.size(), tiles, c.bm,
+                          p->d_err, p->st));
+    }
     if (p->timing) {
       CK(cudaEventRecord(ev[1], p->st));
       CK(cudaEventRecord(ev[2], p->st));
@@ -657,8 +811,12 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     set_error("libpt_plan_create: bad kind/dtype/args");
     return LIBPT_ERR_ARG;
   }
-  if (precision != LIBPT_PREC_FP64) {
+  if (precision != LIBPT_PREC_FP64 && precision != LIBPT_PREC_TF32X3) {
     set_error("libpt_plan_create: unknown precision mode");
+    return LIBPT_ERR_ARG;
+  }
+  if (arena && precision != LIBPT_PREC_FP64) {
+    set_error("libpt_plan_create: the static scratch serves the FP64 path");
     return LIBPT_ERR_ARG;
   }
   const bool unr = kind == 1 || kind == 3, ft = kind >= 2;
@@ -731,6 +889,27 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       break;
     }
     if ((r = add_cases(p))) break;
+    if (p->precision == LIBPT_PREC_TF32X3) {
+      // the tensor-core path reads planes; of the padded FP64 blocks only the
+      // amplitudes stay (the energy epilogue's disconnected term reads them)
+      if (cudaStreamSynchronize(st) != cudaSuccess) {
+        set_error("preparing tensor-core planes failed");
+        r = LIBPT_ERR_CUDA;
+        break;
+      }
+      for (OperandSet *set : {&p->L, &p->R})
+        for (double **q : {&set->ovvv[0], &set->ovvv[1], &set->ovvv[2],
+                           &set->ovvv[3], &set->oovo[0], &set->oovo[1],
+                           &set->oovo[2], &set->oovo[3], &set->taup[0],
+                           &set->taup[1]}) {
+          if (!*q) continue;
+          auto it = std::find(p->allocs.begin(), p->allocs.end(), (void *)*q);
+          if (it != p->allocs.end()) {
+            cudaFree(*q);
+            p->allocs.erase(it);
+          }
+        }
+    }
     if ((r = dalloc(p, (void **)&p->e_slot, (p->queue.size() + 1) * 8))) break;
     if (cudaMemsetAsync(p->e_slot, 0, (p->queue.size() + 1) * 8, st) != cudaSuccess) {
       r = LIBPT_ERR_CUDA;

@@ -18,7 +18,21 @@ void host_free(void *p);
 struct SegT {
   int16_t amap, bmap, neg;
   int8_t aq, ap, bp;
-  int32_t ksteps;
+  int32_t ksteps;   // ceil(k / GEMM_BK) for the DMMA kernel
+  int32_t k;        // contraction length of the segment
+};
+
+// What a map index of a case views: an A operand [P][Q][R][pad4(K)] or a B
+// operand [P][K][Nld] (first N columns meaningful) of padded FP64 data.
+struct OpDesc {
+  int role = -1;    // 0: A, 1: B, -1: unused
+  const double *src = nullptr;
+  int64_t K = 0, R = 0, Q = 0, P = 0, N = 0, Nld = 0;
+};
+
+// TF32 hi/lo planes of one operand, in tensor-core layout.
+struct Planes {
+  float *hi = nullptr, *lo = nullptr;
 };
 
 struct JobT {
@@ -50,6 +64,8 @@ struct SpinCase {
   int ntiles = 0, ctiles = 0;
   double flops_per_triple = 0.0;        // reference GEMM flops
   int bm = GEMM_BM;                     // CTA tile rows of this case's GEMMs
+  OpDesc opd[MAX_MAPS];                 // operand behind each DMMA map
+  TcMapSet tcmaps;                      // tensor-core views (map 2i, 2i+1)
 };
 
 }  // namespace ptb
@@ -84,6 +100,8 @@ struct libpt_plan {
   // is carved from it and nothing is allocated or freed
   char *arena = nullptr;
   size_t arena_size = 0, arena_used = 0;
+  // tensor-core planes, keyed by (source block, role)
+  std::vector<std::pair<std::pair<const double *, int>, ptb::Planes>> planes;
   // kernel timing (libpt_plan_timing): events around each launch
   bool timing = false;
   std::vector<cudaEvent_t> ev_gemm, ev_epi;  // start/stop pairs
@@ -102,6 +120,16 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
 // Device bytes a restricted (T) plan of (o, v) takes from an arena when its
 // batches hold up to nb triples (arena mode, device sources).
 size_t rpt_arena_bytes(int64_t o, int64_t v, int64_t nb);
+// Tensor-core views of TF32 planes (see engine.h): A planes [P][Q][R][Kp],
+// B planes [P][N][Kp] (Kp = pad4(K) floats per row).
+int tc_map_a(CUtensorMap *m, const float *p, int64_t K, int64_t R, int64_t Q,
+             int64_t P);
+int tc_map_b(CUtensorMap *m, const float *p, int64_t K, int64_t N, int64_t P);
+// DMMA views of padded FP64 blocks: A [P][Q][R][pad4(K)], B [P][K][Nld].
+int dmma_map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R,
+               int64_t Q, int64_t P, int bm);
+int dmma_map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld,
+               int64_t K, int64_t P);
 int plan_run(libpt_plan *p, const int64_t *idx, size_t n);
 int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e);
 void plan_destroy(libpt_plan *p);

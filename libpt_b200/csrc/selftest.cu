@@ -1,0 +1,186 @@
+// Built-in self-test of the contraction kernels (libpt_selftest): one job
+// C = A B1 - A B2 with two signed segments on random operands, compared with
+// a plain FP64 product computed on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "plan.h"
+#include "pt.h"
+
+#define LIBPT_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+// Values exactly representable in FP32 (so the TF32 planes split them
+// exactly), uniform in (-1, 1), from an integer hash of (seed, index).
+__global__ void fill_kernel(double *x, int64_t rows, int64_t w, int64_t ld,
+                            uint32_t seed) {
+  const int64_t n = rows * ld;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i % ld;
+    uint32_t h = (uint32_t)i * 2654435761u ^ (seed * 40503u + 0x9e3779b9u);
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    const float u = (float)(h >> 8) * (1.0f / 8388608.0f) - 1.0f;
+    x[i] = c < w ? (double)u : 0.0;
+  }
+}
+
+__global__ void ref_kernel(const double *A, const double *B1, const double *B2,
+                           double *C, int m, int n, int k, int64_t lda,
+                           int64_t ldb) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)m * n) return;
+  const int r = (int)(idx / n), c = (int)(idx % n);
+  double s = 0.0;
+  for (int x = 0; x < k; ++x)
+    s += A[r * lda + x] * (B1[x * ldb + c] - B2[x * ldb + c]);
+  C[r * ldb + c] = s;
+}
+
+}  // namespace
+
+LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
+                             double *rel_err) {
+  using namespace ptb;
+  if (!rel_err || m < 1 || n < 1 || k < 1 || m > 4096 || n > 4096 ||
+      k > 4096 || (precision != LIBPT_PREC_FP64 &&
+                   precision != LIBPT_PREC_TF32X3)) {
+    set_error("libpt_selftest: bad arguments");
+    return LIBPT_ERR_ARG;
+  }
+  const int64_t kp = (k + 3) & ~3, np = (n + 3) & ~3;
+  std::vector<void *> bufs;
+  auto alloc = [&](size_t bytes) -> void * {
+    void *q = nullptr;
+    if (cudaMalloc(&q, bytes) != cudaSuccess) return nullptr;
+    bufs.push_back(q);
+    return q;
+  };
+  auto done = [&](int r) {
+    for (void *q : bufs) cudaFree(q);
+    return r;
+  };
+  double *A = (double *)alloc((size_t)m * kp * 8);
+  double *B1 = (double *)alloc((size_t)k * np * 8);
+  double *B2 = (double *)alloc((size_t)k * np * 8);
+  double *Cm = (double *)alloc((size_t)m * np * 8);
+  double *Cr = (double *)alloc((size_t)m * np * 8);
+  unsigned *err = (unsigned *)alloc(4);
+  GemmJob *dj = (GemmJob *)alloc(sizeof(GemmJob));
+  if (!A || !B1 || !B2 || !Cm || !Cr || !err || !dj) {
+    set_error("libpt_selftest: cudaMalloc failed");
+    return done(LIBPT_ERR_NOMEM);
+  }
+  fill_kernel<<<256, 256>>>(A, m, k, kp, 1);
+  fill_kernel<<<256, 256>>>(B1, k, n, np, 2);
+  fill_kernel<<<256, 256>>>(B2, k, n, np, 3);
+  cudaMemset(Cm, 0, (size_t)m * np * 8);
+  cudaMemset(err, 0, 4);
+  ref_kernel<<<(unsigned)(((int64_t)m * n + 255) / 256), 256>>>(A, B1, B2, Cr, m,
+                                                               n, k, kp, np);
+  GemmJob job;
+  memset(&job, 0, sizeof(job));
+  job.out = Cm;
+  job.ldc = np;
+  job.M = m;
+  job.N = (int)np;
+  job.nseg = 2;
+  int r = LIBPT_OK;
+  cudaError_t ce = cudaSuccess;
+  if (precision == LIBPT_PREC_FP64) {
+    MapSet maps;
+    memset(&maps, 0, sizeof(maps));
+    if ((r = dmma_map_a(&maps.m[0], A, k, m, 1, 1, 128)) ||
+        (r = dmma_map_b(&maps.m[1], B1, n, np, k, 1)) ||
+        (r = dmma_map_b(&maps.m[2], B2, n, np, k, 1)))
+      return done(r);
+    job.mtiles = (m + 127) / 128;
+    job.ntiles_n = (int)((np + GEMM_BN - 1) / GEMM_BN);
+    for (int s = 0; s < 2; ++s) {
+      job.seg[s].amap = 0;
+      job.seg[s].bmap = (int16_t)(1 + s);
+      job.seg[s].neg = (int16_t)s;
+      job.seg[s].ksteps = (k + GEMM_BK - 1) / GEMM_BK;
+    }
+    cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
+    ce = gemm_dmma_launch(maps, dj, 1, job.mtiles * job.ntiles_n, 128, err,
+                          nullptr);
+  } else {
+    float *pl[6];
+    for (int x = 0; x < 6; ++x) {
+      pl[x] = (float *)alloc((size_t)(x < 2 ? m : n) * kp * 4);
+      if (!pl[x]) {
+        set_error("libpt_selftest: cudaMalloc failed");
+        return done(LIBPT_ERR_NOMEM);
+      }
+    }
+    if ((ce = split_tf32_launch(A, pl[0], pl[1], (int64_t)m * kp, nullptr)) ||
+        (ce = transpose_split_tf32_launch(B1, pl[2], pl[3], 1, k, n, np, kp,
+                                          nullptr)) ||
+        (ce = transpose_split_tf32_launch(B2, pl[4], pl[5], 1, k, n, np, kp,
+                                          nullptr))) {
+      set_error(cudaGetErrorString(ce));
+      return done(LIBPT_ERR_CUDA);
+    }
+    TcMapSet maps;
+    memset(&maps, 0, sizeof(maps));
+    for (int x = 0; x < 6; ++x) {
+      r = x < 2 ? tc_map_a(&maps.m[x], pl[x], k, m, 1, 1)
+                : tc_map_b(&maps.m[x], pl[x], k, n, 1);
+      if (r) return done(r);
+    }
+    job.mtiles = (m + TC_BM - 1) / TC_BM;
+    job.ntiles_n = (int)((np + TC_BN - 1) / TC_BN);
+    const int kc = tc_kchunk_elems(TC_TF32);
+    for (int s = 0; s < 2; ++s) {
+      job.seg[s].amap = 0;
+      job.seg[s].bmap = (int16_t)(2 + 2 * s);
+      job.seg[s].neg = (int16_t)s;
+      job.seg[s].ksteps = (k + kc - 1) / kc;
+    }
+    TcProducts pr;
+    memset(&pr, 0, sizeof(pr));
+    const int8_t pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};
+    for (int q = 0; q < 3; ++q) {
+      pr.pa[q] = pa[q];
+      pr.pb[q] = pb[q];
+    }
+    pr.n = 3;
+    cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
+    ce = gemm_tc_launch(TC_TF32, maps, dj, 1, job.mtiles * job.ntiles_n, pr,
+                        err, nullptr);
+  }
+  if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
+  if (ce != cudaSuccess) {
+    set_error(std::string("libpt_selftest: ") + cudaGetErrorString(ce));
+    return done(LIBPT_ERR_CUDA);
+  }
+  unsigned herr = 0;
+  cudaMemcpy(&herr, err, 4, cudaMemcpyDeviceToHost);
+  std::vector<double> hm((size_t)m * np), hr((size_t)m * np);
+  cudaMemcpy(hm.data(), Cm, hm.size() * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(hr.data(), Cr, hr.size() * 8, cudaMemcpyDeviceToHost);
+  double dmax = 0.0, rmax = 0.0;
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < n; ++j) {
+      const size_t x = (size_t)i * np + j;
+      dmax = std::max(dmax, std::fabs(hm[x] - hr[x]));
+      rmax = std::max(rmax, std::fabs(hr[x]));
+    }
+  *rel_err = rmax > 0 ? dmax / rmax : dmax;
+  if (herr) {
+    set_error("libpt_selftest: a device-side wait exceeded its time limit");
+    return done(LIBPT_ERR_TIMEOUT);
+  }
+  return done(LIBPT_OK);
+}

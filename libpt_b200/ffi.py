@@ -21,6 +21,7 @@ LIBPT_OK = 0
 ERRORS = {1: "LIBPT_ERR_ARG", 2: "LIBPT_ERR_NOMEM", 3: "LIBPT_ERR_CUDA",
           4: "LIBPT_ERR_TIMEOUT", 5: "LIBPT_ERR_UNSUPPORTED"}
 PREC_FP64 = 0
+PREC_TF32X3 = 1
 
 _lib = None
 
@@ -83,6 +84,8 @@ def lib():
         vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64),
         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
         ctypes.POINTER(ctypes.c_int64)]
+    L.libpt_selftest.restype = ctypes.c_int
+    L.libpt_selftest.argtypes = [ctypes.c_int] * 4 + [dp]
     L.libpt_plan_destroy.restype = ctypes.c_int
     L.libpt_plan_destroy.argtypes = [vp]
     _lib = L
@@ -122,6 +125,14 @@ def solve_device(case, tensors, mp=False, stream=None):
     ptrs = [ctypes.c_void_p(tensors[n].data_ptr()) for n in args_of(kind)]
     check(f(*_sizes(case), *ptrs, ctypes.c_void_p(stream or 0),
             ctypes.byref(e)))
+    return e.value
+
+
+def selftest(precision, m, n, k):
+    """Relative error of one contraction kernel against an FP64 product
+    (libpt_selftest)."""
+    e = ctypes.c_double(-1.0)
+    check(lib().libpt_selftest(precision, m, n, k, ctypes.byref(e)))
     return e.value
 
 

@@ -1,0 +1,23 @@
+"""GPU self-tests of the contraction kernels (libpt_selftest): one job
+C = A B1 - A B2 (two signed segments) on random operands against an FP64
+product computed on the device, over ragged and tile-aligned shapes."""
+import pytest
+
+from libpt_b200 import ffi
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(128, 256, 32), (1, 1, 1), (5, 7, 3), (200, 300, 100),
+          (477, 1000, 477), (96, 130, 45), (300, 520, 700)]
+
+
+@pytest.mark.parametrize("m,n,k", SHAPES)
+def test_dmma_fp64(m, n, k):
+    assert ffi.selftest(ffi.PREC_FP64, m, n, k) < 1e-13
+
+
+@pytest.mark.parametrize("m,n,k", SHAPES)
+def test_tcgen05_tf32x3(m, n, k):
+    # 3xTF32 keeps ~21 bits per product and the tensor cores accumulate in
+    # FP32: measured 2e-7 .. 1.1e-5 of max|C| for k <= 700
+    assert ffi.selftest(ffi.PREC_TF32X3, m, n, k) < 5e-5

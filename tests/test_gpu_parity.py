@@ -141,3 +141,29 @@ def test_per_triple_energies_match_oracle():
 def test_repeat_is_bitwise_identical():
     case = synth.make("rft", 5, 23, seed=31, fock=1e-3)
     assert ffi.solve_host(case) == ffi.solve_host(case)
+
+
+@pytest.mark.parametrize("name", fixtures.NAMES)
+def test_golden_tf32x3_plan(name, energies):
+    """The 3xTF32 tensor-core form on the golden fixtures (FP32 inputs)."""
+    case = fixtures.load(name)
+    p = ffi.Plan(case, to_dev(case, mp=True), mp=True,
+                 precision=ffi.PREC_TF32X3)
+    p.run()
+    e = p.energy()
+    p.close()
+    assert abs(e - case["e_ref"]) <= GOLDEN_EPS
+
+
+@pytest.mark.parametrize("kind,sz", [("rpt", (6, 40)), ("upt", (4, 23, 3, 25)),
+                                     ("rft", (4, 21)), ("uft", (3, 17, 4, 19))])
+def test_synthetic_tf32x3_plan(kind, sz):
+    """Stated tolerance of the 3xTF32 form: |dE| <= 2e-5 |E|."""
+    case = synth.make(kind, *sz, seed=24, fock=1e-3)
+    ref = oracle.solve(checker(), case)
+    p = ffi.Plan(case, to_dev(case, mp=True), mp=True,
+                 precision=ffi.PREC_TF32X3)
+    p.run()
+    e = p.energy()
+    p.close()
+    assert abs(e - ref) <= 2e-5 * abs(ref)
