@@ -105,6 +105,14 @@ const char *libpt_last_error(void);
                                  sets LIBPT_MP_PRECISION=tf32x3 (otherwise
                                  they evaluate FP32 inputs in FP64)          */
 
+#define LIBPT_PREC_EMU64  2   /* emulated FP64: Ozaki-style split of FP64
+                                 operands into S signed 7-bit digit planes
+                                 (power-of-two scale per row / column), exact
+                                 INT32 accumulation of the S(S+1)/2 leading
+                                 digit products on tcgen05 INT8 tensor cores.
+                                 S = 6 by default; LIBPT_PREC_EMU64 | (S << 8)
+                                 selects S in [4, 7]                          */
+
 /* Built-in self-test of a contraction kernel: C = A B1 - A B2 on random
  * m x k and k x n operands, against an FP64 reference computed on the device;
  * writes max|C - C_ref| / max|C_ref| to *rel_err.  precision selects the

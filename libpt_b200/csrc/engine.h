@@ -41,6 +41,8 @@ struct GemmJob {
   int32_t nseg;
   int32_t mtiles;       // ceil(M / BM); tiles are numbered M-tile fastest
   GemmSeg seg[MAX_SEG];
+  // emulated FP64: power-of-two exponents of the output rows / columns
+  const signed char *ea, *eb;
 };
 
 struct MapSet {
@@ -65,6 +67,10 @@ constexpr int TC_BM = 128;    // rows of a tile (TMEM lanes)
 constexpr int TC_BN = 256;    // columns of a tile
 constexpr int TC_TF32 = 0;    // kinds
 constexpr int TC_INT8 = 1;
+// Emulated FP64: S digit planes per operand, products with p + q <= S - 1
+// (0-based) into S accumulators of TC_I8_BN columns (single buffered).
+constexpr int TC_I8_BN = 64;
+constexpr int TC_S_MIN = 4, TC_S_MAX = 7;
 constexpr int TC_MAX_MAPS = 48;
 
 struct TcMapSet {
@@ -77,10 +83,13 @@ struct TcProducts {           // acc[c] += A_plane[pa] * B_plane[pb]^T
 };
 
 int tc_kchunk_elems(int kind);   // K elements per pipeline stage
+// kind TC_TF32: planes {hi, lo} in separate maps (2i, 2i+1), products from
+// prods.  kind TC_INT8: `slices` digit planes as a coordinate of one map per
+// operand (A maps hold 2*slices planes: the digits, then their negatives).
 cudaError_t gemm_tc_launch(int kind, const TcMapSet &maps,
                            const GemmJob *d_jobs, int njobs, int total_tiles,
                            const TcProducts &prods, unsigned *d_err,
-                           cudaStream_t st);
+                           cudaStream_t st, int slices = 0);
 
 // ---- energy epilogues ------------------------------------------------------
 
@@ -140,5 +149,24 @@ cudaError_t transpose_split_tf32_launch(const double *src, float *hi,
                                         float *lo, int64_t P, int K,
                                         int64_t N, int64_t ldn, int64_t ldk,
                                         cudaStream_t st);
+
+// ---- emulated FP64 preparation (see prep.cu) --------------------------------
+cudaError_t rowmax_launch(const double *src, int64_t npq, int64_t R, int64_t K,
+                          int64_t kp, unsigned long long *rmax,
+                          cudaStream_t st);
+cudaError_t colmax_launch(const double *src, int64_t P, int64_t K, int64_t N,
+                          int64_t w, int64_t wsrc, int64_t ldsrc,
+                          unsigned long long *cmax, cudaStream_t st);
+cudaError_t exps_launch(const unsigned long long *m1,
+                        const unsigned long long *m2, double s2, int64_t n,
+                        signed char *e, cudaStream_t st);
+cudaError_t slice_a_launch(const double *src, int64_t npq, int64_t R,
+                           int64_t K, int64_t kp, int64_t kpi, double scale,
+                           const signed char *ea, int S, signed char *out,
+                           cudaStream_t st);
+cudaError_t slice_b_launch(const double *src, int64_t P, int K, int64_t N,
+                           int64_t w, int64_t wsrc, int64_t ldsrc, int64_t kpi,
+                           double scale, const signed char *eb, int S,
+                           signed char *out, cudaStream_t st);
 
 }  // namespace ptb

@@ -3,19 +3,27 @@
 // Same job/segment structure as gemm_dmma.cu (one triple's contraction
 // output = sum of signed amplitude x integral products), but the products
 // run on the 5th-generation tensor cores with accumulators in TMEM.  Each
-// operand is stored as PA (A side) / PB (B side) "planes" -- e.g. the high
-// and low TF32 parts of an FP32 value -- and a tile's result is
-//     acc[c] = sum over the products (pa, pb, c) of A_plane[pa] * B_plane[pb]^T
-// combined by the epilogue into FP64.  3xTF32: planes {hi, lo}, products
-// hi*hi + hi*lo + lo*hi into one FP32 accumulator (the *_mp entry points).
+// operand is stored as NPL "planes", and a tile's result is assembled from
+// plane products accumulated in TMEM:
+//
+//  * TF32 (3xTF32, FP32-level): planes {hi, lo} of FP32 values, products
+//    hi*hi + hi*lo + lo*hi into one FP32 accumulator; the MMA's negate bit
+//    applies a segment's sign.
+//  * INT8 (emulated FP64, Ozaki-style): planes = S signed 7-bit digits of
+//    the operand scaled by a power of two per row (A) / column (B); the
+//    products d^A_p d^B_q with p + q <= S-1 are summed exactly in INT32, one
+//    accumulator per digit weight 2^-7(p+q+2), and the epilogue forms
+//       C = 2^(ea[row] + eb[col]) * sum_w acc_w 2^-7(w+2)        in FP64.
+//    Subtracted segments read the negated digit planes (A planes S..2S-1).
 //
 // Warp roles (persistent CTA, one per SM):
-//   warp 0      TMA producer: A and B plane tiles of one 128-byte K chunk per
-//               pipeline stage (128B-swizzled, K-major)
+//   warp 0      TMA producer: A and B plane tiles of one K chunk per stage
+//               (swizzled, K-major)
 //   warp 1      TMEM owner and MMA issuer: one thread issues tcgen05.mma for
-//               every product and K step, tcgen05.commit frees the stage
-//   warps 2-5   epilogue: tcgen05.ld of the finished accumulator (double
-//               buffered in TMEM so the next tile's MMAs overlap), FP64 store
+//               every product and K step; tcgen05.commit frees the stage
+//   warps 2-5   epilogue: tcgen05.ld of the finished accumulators, FP64
+//               store (TF32: accumulators double buffered in TMEM so the
+//               next tile's MMAs overlap the drain)
 // All mbarrier waits are bounded; on expiry the kernel records the error,
 // stops issuing, still releases TMEM, and returns.
 #include "common.cuh"
@@ -25,8 +33,7 @@ namespace ptb {
 
 namespace {
 
-constexpr int BM = TC_BM;          // 128 rows (TMEM lanes)
-constexpr int KCHUNK = 128;        // bytes of K per stage (one swizzle row)
+constexpr int BM = TC_BM;   // 128 rows (TMEM lanes)
 
 __device__ __forceinline__ int find_job(const GemmJob *jobs, int njobs,
                                         int tile) {
@@ -41,12 +48,14 @@ __device__ __forceinline__ int find_job(const GemmJob *jobs, int njobs,
   return lo;
 }
 
-// Shared-memory matrix descriptor, K-major operand in 128B-swizzled rows of
-// 128 bytes, 8-row core groups 1024 bytes apart (SBO), sm_100 version 1.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+// Shared-memory matrix descriptor of a K-major operand stored as SW-byte
+// swizzled rows (8-row core groups SW*8 bytes apart), sm_100 version 1.
+template <int SW>
+__device__ __forceinline__ uint64_t kmajor_desc(uint32_t saddr) {
+  constexpr uint64_t layout = SW == 128 ? 2 : SW == 64 ? 4 : 6;
   return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) |
-         ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) |
-         ((uint64_t)2 << 61);
+         ((uint64_t)((SW * 8) >> 4) << 32) | ((uint64_t)1 << 46) |
+         (layout << 61);
 }
 
 __device__ __forceinline__ void tc_fence_before() {
@@ -106,31 +115,37 @@ __host__ __device__ constexpr uint32_t tc_idesc() {
          ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
-template <int KIND, int BN, int PA, int PB, int NACC, int ST>
+constexpr int pow2_cols(int c) {
+  return c <= 32 ? 32 : c <= 64 ? 64 : c <= 128 ? 128 : c <= 256 ? 256 : 512;
+}
+
+template <int KIND, int BN, int NPL, int NACC, int ST, int SW, int NBUF>
 struct TcCfg {
-  static constexpr int A_TILE = BM * KCHUNK;      // bytes per A plane tile
-  static constexpr int B_TILE = BN * KCHUNK;      // bytes per B plane tile
-  static constexpr int STAGE = PA * A_TILE + PB * B_TILE;
+  static constexpr int A_TILE = BM * SW;          // bytes per A plane tile
+  static constexpr int B_TILE = BN * SW;          // bytes per B plane tile
+  static constexpr int STAGE = NPL * (A_TILE + B_TILE);
   static constexpr int KSTEP = 32;                // bytes of K per MMA
-  static constexpr int TMEM_COLS = 2 * NACC * BN; // double-buffered accumulators
+  static constexpr int KELEM = KIND == TC_TF32 ? SW / 4 : SW;
+  static constexpr int TMEM_COLS = pow2_cols(NBUF * NACC * BN);
   static constexpr int SMEM = ST * STAGE + 1024 /*align*/ + 256 /*barriers*/;
-  static_assert(TMEM_COLS <= 512, "TMEM holds 512 columns");
+  static_assert(NBUF * NACC * BN <= 512, "TMEM holds 512 columns");
+  static_assert(STAGE % 1024 == 0, "stage tiles keep 1 KiB alignment");
 };
 
-template <int KIND, int BN, int PA, int PB, int NACC, int ST>
+template <int KIND, int BN, int NPL, int NACC, int ST, int SW, int NBUF>
 __global__ void __launch_bounds__(192, 1)
     gemm_tc_kernel(const __grid_constant__ TcMapSet maps,
                    const GemmJob *__restrict__ jobs, int njobs,
                    int total_tiles, const __grid_constant__ TcProducts prods,
                    unsigned *err) {
-  using C = TcCfg<KIND, BN, PA, PB, NACC, ST>;
+  using C = TcCfg<KIND, BN, NPL, NACC, ST, SW, NBUF>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   unsigned char *smem = smem_raw + ((1024 - (raw & 1023)) & 1023);
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + ST * C::STAGE);
   uint64_t *empty = full + ST;
-  uint64_t *accfull = empty + ST;      // [2]
-  uint64_t *accempty = accfull + 2;    // [2]
+  uint64_t *accfull = empty + ST;      // [NBUF]
+  uint64_t *accempty = accfull + 2;    // [NBUF]
   uint32_t *taddr_s = reinterpret_cast<uint32_t *>(accempty + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -139,7 +154,7 @@ __global__ void __launch_bounds__(192, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NBUF; ++b) {
       mbar_init(&accfull[b], 1);
       mbar_init(&accempty[b], 128);
     }
@@ -176,15 +191,22 @@ __global__ void __launch_bounds__(192, 1)
           }
           mbar_arrive_expect_tx(&full[stage], C::STAGE);
           unsigned char *st_base = smem + stage * C::STAGE;
-          const int k0 = ks * (KIND == TC_TF32 ? KCHUNK / 4 : KCHUNK);
+          const int k0 = ks * C::KELEM;
 #pragma unroll
-          for (int p = 0; p < PA; ++p)
-            tma_load_4d(st_base + p * C::A_TILE, &maps.m[sg.amap + p],
-                        &full[stage], k0, m0, sg.a_q, sg.a_p);
-#pragma unroll
-          for (int p = 0; p < PB; ++p)
-            tma_load_3d(st_base + PA * C::A_TILE + p * C::B_TILE,
-                        &maps.m[sg.bmap + p], &full[stage], k0, n0, sg.b_p);
+          for (int p = 0; p < NPL; ++p) {
+            if (KIND == TC_TF32) {
+              tma_load_4d(st_base + p * C::A_TILE, &maps.m[sg.amap + p],
+                          &full[stage], k0, m0, sg.a_q, sg.a_p);
+              tma_load_3d(st_base + NPL * C::A_TILE + p * C::B_TILE,
+                          &maps.m[sg.bmap + p], &full[stage], k0, n0, sg.b_p);
+            } else {
+              tma_load_5d(st_base + p * C::A_TILE, &maps.m[sg.amap],
+                          &full[stage], k0, m0, sg.a_q, sg.a_p,
+                          p + (sg.neg ? NPL : 0));
+              tma_load_4d(st_base + NPL * C::A_TILE + p * C::B_TILE,
+                          &maps.m[sg.bmap], &full[stage], k0, n0, sg.b_p, p);
+            }
+          }
           if (++stage == ST) {
             stage = 0;
             phase ^= 1u;
@@ -201,8 +223,10 @@ __global__ void __launch_bounds__(192, 1)
     for (int tile = blockIdx.x; tile < total_tiles && ok;
          tile += gridDim.x, ++it) {
       const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
-      const int ab = it & 1;
-      if (!mbar_wait(&accempty[ab], (uint32_t)(((it >> 1) & 1) ^ 1), err)) {
+      const int ab = NBUF == 2 ? (it & 1) : 0;
+      const uint32_t epar = NBUF == 2 ? (uint32_t)(((it >> 1) & 1) ^ 1)
+                                      : (uint32_t)((it & 1) ^ 1);
+      if (!mbar_wait(&accempty[ab], epar, err)) {
         ok = false;
         break;
       }
@@ -219,21 +243,39 @@ __global__ void __launch_bounds__(192, 1)
           }
           tc_fence_after();
           const uint32_t sa = smem_u32(smem + stage * C::STAGE);
-          const uint32_t sb = sa + PA * C::A_TILE;
-          for (int q = 0; q < prods.n; ++q) {
-            const int c = prods.acc[q];
-            const uint64_t da = sw128_desc(sa + prods.pa[q] * C::A_TILE);
-            const uint64_t db = sw128_desc(sb + prods.pb[q] * C::B_TILE);
-            const uint32_t tm = acc0 + (uint32_t)(c * BN);
+          const uint32_t sb = sa + NPL * C::A_TILE;
+          if (KIND == TC_TF32) {
+            for (int q = 0; q < prods.n; ++q) {
+              const int c = prods.acc[q];
+              const uint64_t da = kmajor_desc<SW>(sa + prods.pa[q] * C::A_TILE);
+              const uint64_t db = kmajor_desc<SW>(sb + prods.pb[q] * C::B_TILE);
 #pragma unroll
-            for (int kk = 0; kk < KCHUNK / C::KSTEP; ++kk) {
-              // advancing the start address by 32 B steps through the
-              // swizzled 128-byte row (K-major SW128 layout)
-              tc_mma<KIND>(tm, da + (uint64_t)(kk * C::KSTEP >> 4),
-                           db + (uint64_t)(kk * C::KSTEP >> 4),
-                           tc_idesc<KIND, BN>() | neg,
-                           (started >> c) & 1u);
-              started |= 1u << c;
+              for (int kk = 0; kk < SW / C::KSTEP; ++kk) {
+                // 32-byte K steps through the swizzled row (K-major layout)
+                tc_mma<KIND>(acc0 + (uint32_t)(c * BN),
+                             da + (uint64_t)(kk * C::KSTEP >> 4),
+                             db + (uint64_t)(kk * C::KSTEP >> 4),
+                             tc_idesc<KIND, BN>() | neg, (started >> c) & 1u);
+                started |= 1u << c;
+              }
+            }
+          } else {
+#pragma unroll
+            for (int pa = 0; pa < NPL; ++pa) {
+              const uint64_t da = kmajor_desc<SW>(sa + pa * C::A_TILE);
+#pragma unroll
+              for (int pb = 0; pb + pa < NPL; ++pb) {
+                const int c = pa + pb;     // digit weight 2^-7(c+2)
+                const uint64_t db = kmajor_desc<SW>(sb + pb * C::B_TILE);
+#pragma unroll
+                for (int kk = 0; kk < SW / C::KSTEP; ++kk) {
+                  tc_mma<KIND>(acc0 + (uint32_t)(c * BN),
+                               da + (uint64_t)(kk * C::KSTEP >> 4),
+                               db + (uint64_t)(kk * C::KSTEP >> 4),
+                               tc_idesc<KIND, BN>(), (started >> c) & 1u);
+                  started |= 1u << c;
+                }
+              }
             }
           }
           tc_commit(&empty[stage]);   // stage reusable once these MMAs finish
@@ -254,36 +296,48 @@ __global__ void __launch_bounds__(192, 1)
       const int local = tile - job.tile_begin;
       const int m0 = (local % job.mtiles) * BM;
       const int n0 = (local / job.mtiles) * BN;
-      const int ab = it & 1;
-      if (!mbar_wait(&accfull[ab], (uint32_t)((it >> 1) & 1), err)) break;
+      const int ab = NBUF == 2 ? (it & 1) : 0;
+      const uint32_t fpar = NBUF == 2 ? (uint32_t)((it >> 1) & 1)
+                                      : (uint32_t)(it & 1);
+      if (!mbar_wait(&accfull[ab], fpar, err)) break;
       tc_fence_after();
       const int row = m0 + 32 * q + lane;
       double *orow = job.out + (int64_t)row * job.ldc;
+      const int erow = (KIND == TC_INT8 && row < job.M) ? job.ea[row] : 0;
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) +
                              (uint32_t)(ab * NACC * BN);
 #pragma unroll 1
       for (int c0 = 0; c0 < BN; c0 += 32) {
-        uint32_t r[NACC][32];
+        double v[32];
+        uint32_t r[32];
+        if (KIND == TC_TF32) {
+          tmem_ld32(tbase + c0, r);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int a = 0; a < NACC; ++a) tmem_ld32(tbase + a * BN + c0, r[a]);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          for (int x = 0; x < 32; ++x) v[x] = (double)__uint_as_float(r[x]);
+        } else {
+          // exact integers scaled by powers of two, summed from the smallest
+          // digit weight up
+#pragma unroll
+          for (int x = 0; x < 32; ++x) v[x] = 0.0;
+#pragma unroll 1
+          for (int a = NACC - 1; a >= 0; --a) {
+            tmem_ld32(tbase + a * BN + c0, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int x = 0; x < 32; ++x)
+              v[x] += ldexp((double)(int)r[x], -7 * (a + 2));
+          }
+        }
         if (row < job.M) {
 #pragma unroll
           for (int x = 0; x < 32; x += 2) {
             const int col = n0 + c0 + x;
             if (col < job.N) {
-              double v0, v1;
-              if (KIND == TC_TF32) {
-                v0 = (double)__uint_as_float(r[0][x]);
-                v1 = (double)__uint_as_float(r[0][x + 1]);
-              } else {
-                v0 = 0.0;
-                v1 = 0.0;
-#pragma unroll
-                for (int a = 0; a < NACC; ++a) {
-                  v0 += ldexp((double)(int)r[a][x], -7 * (a + 2));
-                  v1 += ldexp((double)(int)r[a][x + 1], -7 * (a + 2));
-                }
+              double v0 = v[x], v1 = v[x + 1];
+              if (KIND == TC_INT8) {
+                v0 = ldexp(v0, erow + job.eb[col]);
+                v1 = ldexp(v1, erow + job.eb[col + 1]);
               }
               *reinterpret_cast<double2 *>(orow + col) = make_double2(v0, v1);
             }
@@ -305,13 +359,13 @@ __global__ void __launch_bounds__(192, 1)
   }
 }
 
-template <int KIND, int BN, int PA, int PB, int NACC, int ST>
+template <int KIND, int BN, int NPL, int NACC, int ST, int SW, int NBUF>
 cudaError_t launch(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
                    int total_tiles, const TcProducts &prods, unsigned *d_err,
                    cudaStream_t st) {
-  using C = TcCfg<KIND, BN, PA, PB, NACC, ST>;
+  using C = TcCfg<KIND, BN, NPL, NACC, ST, SW, NBUF>;
   static bool configured = false;
-  auto kern = gemm_tc_kernel<KIND, BN, PA, PB, NACC, ST>;
+  auto kern = gemm_tc_kernel<KIND, BN, NPL, NACC, ST, SW, NBUF>;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(
         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
@@ -324,19 +378,38 @@ cudaError_t launch(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
   return cudaGetLastError();
 }
 
+// Emulated FP64 with S digit planes: 64-byte K chunks, stages as many as fit.
+template <int S>
+cudaError_t launch_i8(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
+                      int total_tiles, const TcProducts &prods,
+                      unsigned *d_err, cudaStream_t st) {
+  constexpr int STAGE = S * (TC_BM + TC_I8_BN) * 64;
+  constexpr int NST = (227 * 1024 - 1024 - 256) / STAGE;
+  static_assert(NST >= 2, "two pipeline stages at least");
+  return launch<TC_INT8, TC_I8_BN, S, S, (NST > 4 ? 4 : NST), 64, 1>(
+      maps, d_jobs, njobs, total_tiles, prods, d_err, st);
+}
+
 }  // namespace
 
-int tc_kchunk_elems(int kind) { return kind == TC_TF32 ? KCHUNK / 4 : KCHUNK; }
+int tc_kchunk_elems(int kind) { return kind == TC_TF32 ? 32 : 64; }
 
 cudaError_t gemm_tc_launch(int kind, const TcMapSet &maps,
                            const GemmJob *d_jobs, int njobs, int total_tiles,
                            const TcProducts &prods, unsigned *d_err,
-                           cudaStream_t st) {
+                           cudaStream_t st, int slices) {
   if (total_tiles <= 0) return cudaSuccess;
   if (kind == TC_TF32)
-    return launch<TC_TF32, TC_BN, 2, 2, 1, 2>(maps, d_jobs, njobs, total_tiles,
-                                              prods, d_err, st);
-  return cudaErrorInvalidValue;
+    return launch<TC_TF32, TC_BN, 2, 1, 2, 128, 2>(maps, d_jobs, njobs,
+                                                   total_tiles, prods, d_err,
+                                                   st);
+  switch (slices) {
+    case 4: return launch_i8<4>(maps, d_jobs, njobs, total_tiles, prods, d_err, st);
+    case 5: return launch_i8<5>(maps, d_jobs, njobs, total_tiles, prods, d_err, st);
+    case 6: return launch_i8<6>(maps, d_jobs, njobs, total_tiles, prods, d_err, st);
+    case 7: return launch_i8<7>(maps, d_jobs, njobs, total_tiles, prods, d_err, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace ptb

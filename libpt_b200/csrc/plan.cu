@@ -144,6 +144,58 @@ int dalloc(libpt_plan *p, void **ptr, size_t bytes);
 
 }  // namespace
 
+int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
+             int64_t Q, int64_t P, int S) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return LIBPT_ERR_CUDA;
+  }
+  const int64_t kpi = (K + 15) & ~int64_t(15);
+  cuuint64_t dims[5] = {(cuuint64_t)K, (cuuint64_t)R, (cuuint64_t)Q,
+                        (cuuint64_t)P, (cuuint64_t)(2 * S)};
+  cuuint64_t str[4] = {(cuuint64_t)kpi, (cuuint64_t)(R * kpi),
+                       (cuuint64_t)(Q * R * kpi), (cuuint64_t)(P * Q * R * kpi)};
+  cuuint32_t box[5] = {64, (cuuint32_t)TC_BM, 1, 1, 1};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, (void *)p, dims, str,
+                   box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (INT8 A view) failed: " +
+              std::to_string(r));
+    return LIBPT_ERR_CUDA;
+  }
+  return LIBPT_OK;
+}
+
+int i8_map_b(CUtensorMap *m, const signed char *p, int64_t K, int64_t N,
+             int64_t P, int S) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return LIBPT_ERR_CUDA;
+  }
+  const int64_t kpi = (K + 15) & ~int64_t(15);
+  cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)N, (cuuint64_t)P,
+                        (cuuint64_t)S};
+  cuuint64_t str[3] = {(cuuint64_t)kpi, (cuuint64_t)(N * kpi),
+                       (cuuint64_t)(P * N * kpi)};
+  cuuint32_t box[4] = {64, (cuuint32_t)TC_I8_BN, 1, 1};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, (void *)p, dims, str,
+                   box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled (INT8 B view) failed: " +
+              std::to_string(r));
+    return LIBPT_ERR_CUDA;
+  }
+  return LIBPT_OK;
+}
+
 int dmma_map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R,
                int64_t Q, int64_t P, int bm) {
   return map_a(m, p, K, R, Q, P, bm);
@@ -353,15 +405,23 @@ int upload_set(libpt_plan *p, Uploader &up, const Sizes &S, OperandSet &set,
       return r;
     off_o += S.oovo(b);
     S.ovvv_shape(b, rows, w);
-    if (dalloc(p, (void **)&set.ovvv[b], rows * pad4(w) * 8)) return LIBPT_ERR_NOMEM;
-    if (int r = up.put(set.ovvv[b], (const char *)ovvv + off_v * es, rows, w, pad4(w)))
-      return r;
+    if (p->precision == LIBPT_PREC_EMU64 && !up.host && !up.fp32) {
+      // sliced in place from the caller's device block: no FP64 copy
+      set.ovvv_src[b] = (const double *)ovvv + off_v;
+    } else {
+      if (dalloc(p, (void **)&set.ovvv[b], rows * pad4(w) * 8))
+        return LIBPT_ERR_NOMEM;
+      if (int r = up.put(set.ovvv[b], (const char *)ovvv + off_v * es, rows, w,
+                         pad4(w)))
+        return r;
+    }
     off_v += S.ovvv(b);
   }
   if (!p->unrestricted) {   // src/pt.c:471-473: baba blocks alias abab
     set.tau[3] = set.tau[1];
     set.oovo[3] = set.oovo[1];
     set.ovvv[3] = set.ovvv[1];
+    set.ovvv_src[3] = set.ovvv_src[1];
   }
   // packed-pair copies of the same-spin amplitudes
   for (int s = 0; s < (p->unrestricted ? 2 : 1); ++s) {
@@ -389,9 +449,10 @@ SegT seg(int amap, int bmap, bool neg, int aq, int ap, int bp, int64_t k) {
 
 enum { I = 0, J = 1, K = 2 };
 
-// Encode a DMMA view and remember what it views (for the tensor-core path).
-int reg_a(SpinCase &c, int idx, const double *ptr, int64_t Kd, int64_t R,
-          int64_t Q, int64_t P) {
+// Encode a DMMA view (FP64 path) and remember what it views, for the
+// tensor-core paths; fam/part classify the operand for emulated FP64.
+int reg_a(libpt_plan *p, SpinCase &c, int idx, const double *ptr, int64_t Kd,
+          int64_t R, int64_t Q, int64_t P, int fam, int part) {
   OpDesc &d = c.opd[idx];
   d.role = 0;
   d.src = ptr;
@@ -399,11 +460,18 @@ int reg_a(SpinCase &c, int idx, const double *ptr, int64_t Kd, int64_t R,
   d.R = R;
   d.Q = Q;
   d.P = P;
+  d.fam = fam;
+  d.part = part;
+  if (p->precision != LIBPT_PREC_FP64) return LIBPT_OK;
   return map_a(&c.maps.m[idx], ptr, Kd, R, Q, P, c.bm);
 }
 
-int reg_b(SpinCase &c, int idx, const double *ptr, int64_t N, int64_t Nld,
-          int64_t Kd, int64_t P) {
+// B operand [P][K][N] in the engine's padded layout (row length Nld), or --
+// when src_w > 0 -- the caller's unpadded pt.h block whose N index is
+// row-padded: n = y*src_w + c, c < src_wsrc real, rows of src_ld elements.
+int reg_b(libpt_plan *p, SpinCase &c, int idx, const double *ptr, int64_t N,
+          int64_t Nld, int64_t Kd, int64_t P, int fam, int part,
+          int64_t src_ld = 0, int64_t src_w = 0, int64_t src_wsrc = 0) {
   OpDesc &d = c.opd[idx];
   d.role = 1;
   d.src = ptr;
@@ -411,7 +479,53 @@ int reg_b(SpinCase &c, int idx, const double *ptr, int64_t N, int64_t Nld,
   d.N = N;
   d.Nld = Nld;
   d.P = P;
+  d.fam = fam;
+  d.part = part;
+  if (src_w > 0) {
+    d.ldsrc = src_ld;
+    d.w = src_w;
+    d.wsrc = src_wsrc;
+  } else {
+    d.ldsrc = Nld;
+    d.w = Nld;
+    d.wsrc = Nld;
+  }
+  if (p->precision != LIBPT_PREC_FP64) return LIBPT_OK;
   return map_b(&c.maps.m[idx], ptr, N, Nld, Kd, P);
+}
+
+// Scale families of emulated FP64: the A operands of a job (amplitude and
+// OOVO blocks of one spin-block index) and its B operands (OVVV block and
+// the amplitude block of the same index) share row / column scales.
+int fam_a(const libpt_plan *p, int set, int b) {
+  return set * 8 + (!p->unrestricted && b == 3 ? 1 : b);
+}
+int fam_b(const libpt_plan *p, int set, int b) {
+  return 100 + set * 8 + (!p->unrestricted && b == 3 ? 1 : b);
+}
+
+// OVVV block b of a set as a B operand: the padded FP64 copy, or the
+// caller's pt.h block when it is sliced in place (emulated FP64, device
+// inputs).  N counts the padded-convention columns.
+int reg_ovvv(libpt_plan *p, SpinCase &c, int idx, const OperandSet &S, int b,
+             int64_t N, int64_t Nld, int64_t Kd, int64_t P, int fam) {
+  if (S.ovvv[b])
+    return reg_b(p, c, idx, S.ovvv[b], N, Nld, Kd, P, fam, 0);
+  const int64_t va = p->va, vb = p->vb;
+  int64_t ld, w, wsrc;
+  if (b == 0 || b == 2) {   // packed pairs: no inner padding
+    const int64_t v = b ? vb : va;
+    ld = w = wsrc = v * (v - 1) / 2;
+  } else if (b == 1) {      // [oa][vb][va][vb]: N = (y < va, c < vb)
+    ld = va * vb;
+    w = pad4(vb);
+    wsrc = vb;
+  } else {                  // [ob][va][vb][va]
+    ld = vb * va;
+    w = pad4(va);
+    wsrc = va;
+  }
+  return reg_b(p, c, idx, S.ovvv_src[b], N, Nld, Kd, P, fam, 0, ld, w, wsrc);
 }
 
 // Same-spin case: four maps per operand set, one job (T) per set.
@@ -428,10 +542,12 @@ int build_aaa(libpt_plan *p, SpinCase &c) {
   for (int x = 0; x < nset; ++x) {
     const OperandSet &set = x ? p->R : p->L;
     const int b0 = 4 * x;
-    if (int r = reg_a(c, b0 + 0, set.tau[s ? 2 : 0], v, v, o, o)) return r;
-    if (int r = reg_a(c, b0 + 1, set.oovo[s ? 2 : 0], o, v, o, o)) return r;
-    if (int r = reg_b(c, b0 + 2, set.ovvv[s ? 2 : 0], np, ldT, v, o)) return r;
-    if (int r = reg_b(c, b0 + 3, set.taup[s], np, ldT, o, o)) return r;
+    const int bi = s ? 2 : 0;
+    const int fa = fam_a(p, x, bi), fb = fam_b(p, x, bi);
+    if (int r = reg_a(p, c, b0 + 0, set.tau[bi], v, v, o, o, fa, 0)) return r;
+    if (int r = reg_a(p, c, b0 + 1, set.oovo[bi], o, v, o, o, fa, 1)) return r;
+    if (int r = reg_ovvv(p, c, b0 + 2, set, bi, np, ldT, v, o, fb)) return r;
+    if (int r = reg_b(p, c, b0 + 3, set.taup[s], np, ldT, o, o, fb, 1)) return r;
     JobT j;
     j.off = offs[x];
     j.M = (int)v;
@@ -514,18 +630,22 @@ int build_aab(libpt_plan *p, SpinCase &c) {
     const OperandSet &S = x ? p->R : p->L;
     const int m = 12 * x;
     int r;
-    if ((r = reg_a(c, m + 0, S.tau[Taa], va, va, oa, oa))) return r;
-    if ((r = reg_a(c, m + 1, S.tau[Tab], vb, va, ob, oa))) return r;
-    if ((r = reg_a(c, m + 2, S.tau[Tba], va, vb, oa, ob))) return r;
-    if ((r = reg_a(c, m + 3, S.oovo[Taa], oa, va, oa, oa))) return r;
-    if ((r = reg_a(c, m + 4, S.oovo[Tab], ob, va, ob, oa))) return r;
-    if ((r = reg_a(c, m + 5, S.oovo[Tba], oa, vb, oa, ob))) return r;
-    if ((r = reg_b(c, m + 6, S.ovvv[Taa], np, ldP, va, oa))) return r;
-    if ((r = reg_b(c, m + 7, S.ovvv[Tab], ld1, ld1, vb, oa))) return r;
-    if ((r = reg_b(c, m + 8, S.ovvv[Tba], ld2, ld2, va, ob))) return r;
-    if ((r = reg_b(c, m + 9, S.taup[f], np, ldP, oa, oa))) return r;
-    if ((r = reg_b(c, m + 10, S.tau[Tab], ld1, ld1, ob, oa))) return r;
-    if ((r = reg_b(c, m + 11, S.tau[Tba], ld2, ld2, oa, ob))) return r;
+    const int A0 = fam_a(p, x, Taa), A1 = fam_a(p, x, Tab),
+              A3 = fam_a(p, x, Tba);
+    const int B0 = fam_b(p, x, Taa), B1 = fam_b(p, x, Tab),
+              B3 = fam_b(p, x, Tba);
+    if ((r = reg_a(p, c, m + 0, S.tau[Taa], va, va, oa, oa, A0, 0))) return r;
+    if ((r = reg_a(p, c, m + 1, S.tau[Tab], vb, va, ob, oa, A1, 0))) return r;
+    if ((r = reg_a(p, c, m + 2, S.tau[Tba], va, vb, oa, ob, A3, 0))) return r;
+    if ((r = reg_a(p, c, m + 3, S.oovo[Taa], oa, va, oa, oa, A0, 1))) return r;
+    if ((r = reg_a(p, c, m + 4, S.oovo[Tab], ob, va, ob, oa, A1, 1))) return r;
+    if ((r = reg_a(p, c, m + 5, S.oovo[Tba], oa, vb, oa, ob, A3, 1))) return r;
+    if ((r = reg_ovvv(p, c, m + 6, S, Taa, np, ldP, va, oa, B0))) return r;
+    if ((r = reg_ovvv(p, c, m + 7, S, Tab, ld1, ld1, vb, oa, B1))) return r;
+    if ((r = reg_ovvv(p, c, m + 8, S, Tba, ld2, ld2, va, ob, B3))) return r;
+    if ((r = reg_b(p, c, m + 9, S.taup[f], np, ldP, oa, oa, B0, 1))) return r;
+    if ((r = reg_b(p, c, m + 10, S.tau[Tab], ld1, ld1, ob, oa, B1, 1))) return r;
+    if ((r = reg_b(p, c, m + 11, S.tau[Tba], ld2, ld2, oa, ob, B3, 1))) return r;
     const int b = 12 * x;
     JobT u1, u2, pp;
     // U1[x][y,c] = -t_ik I_j + t_jk I_i + O_jk t_i - O_ik t_j
@@ -615,6 +735,123 @@ int build_aab(libpt_plan *p, SpinCase &c) {
   return LIBPT_OK;
 }
 
+Family *family(libpt_plan *p, int id, int64_t n) {
+  for (Family &f : p->fams)
+    if (f.id == id) return &f;
+  Family f;
+  f.id = id;
+  f.n = n;
+  if (dalloc(p, (void **)&f.max0, n * 8 + 8) ||
+      dalloc(p, (void **)&f.max1, n * 8 + 8) || dalloc(p, (void **)&f.e, n + 16))
+    return nullptr;
+  cudaMemsetAsync(f.max0, 0, n * 8 + 8, p->st);
+  cudaMemsetAsync(f.max1, 0, n * 8 + 8, p->st);
+  p->fams.push_back(f);
+  return &p->fams.back();
+}
+
+// Emulated FP64, phase 1: per-row / per-column maxima of every operand of
+// every case, into its family's part (each operand once).
+int i8_maxima(libpt_plan *p) {
+  std::vector<std::pair<const double *, int>> seen;
+  for (SpinCase &c : p->cases) {
+    if (c.count == 0) continue;
+    for (int i = 0; i < MAX_MAPS; ++i) {
+      const OpDesc &d = c.opd[i];
+      if (d.role < 0) continue;
+      Family *f = family(p, d.fam, d.role == 0 ? d.R : d.N);
+      if (!f) return LIBPT_ERR_NOMEM;
+      const std::pair<const double *, int> key(d.src, d.role * 2 + d.part);
+      if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
+      seen.push_back(key);
+      unsigned long long *m = d.part ? f->max1 : f->max0;
+      if (d.role == 0)
+        CK(rowmax_launch(d.src, d.P * d.Q, d.R, d.K, pad4(d.K), m, p->st));
+      else
+        CK(colmax_launch(d.src, d.P, d.K, d.N, d.w, d.wsrc, d.ldsrc, m, p->st));
+    }
+  }
+  return LIBPT_OK;
+}
+
+// Phase 2: per operand set, the power-of-two exchange between the OOVO and
+// the amplitude operand sides that balances their magnitudes; phase 3: the
+// joint exponents of every family.
+int i8_exponents(libpt_plan *p) {
+  std::vector<unsigned long long> h;
+  for (int x = 0; x < (p->ft ? 2 : 1); ++x) {
+    double m0 = 0.0, m1 = 0.0;
+    for (Family &f : p->fams) {
+      if (f.id >= 100 || f.id / 8 != x) continue;   // A families of set x
+      for (int part = 0; part < 2; ++part) {
+        h.assign(f.n, 0);
+        CK(cudaMemcpyAsync(h.data(), part ? f.max1 : f.max0, f.n * 8,
+                           cudaMemcpyDeviceToHost, p->st));
+        CK(cudaStreamSynchronize(p->st));
+        for (unsigned long long u : h) {
+          double v;
+          memcpy(&v, &u, 8);
+          (part ? m1 : m0) = std::max(part ? m1 : m0, v);
+        }
+      }
+    }
+    OperandSet &S = x ? p->R : p->L;
+    S.balance = (m0 > 0 && m1 > 0) ? (int)std::lround(std::log2(m1 / m0)) : 0;
+  }
+  for (Family &f : p->fams) {
+    const int set = (f.id % 100) / 8;
+    const int k = (set ? p->R : p->L).balance;
+    const double s1 = std::ldexp(1.0, f.id >= 100 ? k : -k);
+    CK(exps_launch(f.max0, f.max1, s1, f.n, f.e, p->st));
+  }
+  return LIBPT_OK;
+}
+
+// Phase 4: digit planes of every operand and the INT8 tensor-core views.
+int i8_planes(libpt_plan *p, SpinCase &c) {
+  const int S = p->slices;
+  for (int i = 0; i < MAX_MAPS; ++i) {
+    const OpDesc &d = c.opd[i];
+    if (d.role < 0) continue;
+    Family *f = family(p, d.fam, d.role == 0 ? d.R : d.N);
+    if (!f) return LIBPT_ERR_NOMEM;
+    const int set = (d.fam % 100) / 8;
+    const int k = (set ? p->R : p->L).balance;
+    const int64_t kpi = (d.K + 15) & ~int64_t(15);
+    const std::pair<const double *, int> key(d.src, d.role);
+    signed char *pl = nullptr;
+    for (auto &e : p->i8planes)
+      if (e.first == key) pl = e.second;
+    if (!pl) {
+      if (d.role == 0) {
+        const int64_t n = d.P * d.Q * d.R * kpi;
+        if (dalloc(p, (void **)&pl, 2 * S * n)) return LIBPT_ERR_NOMEM;
+        CK(slice_a_launch(d.src, d.P * d.Q, d.R, d.K, pad4(d.K), kpi,
+                          std::ldexp(1.0, d.part ? -k : 0), f->e, S, pl,
+                          p->st));
+      } else {
+        const int64_t n = d.P * d.N * kpi;
+        if (dalloc(p, (void **)&pl, S * n)) return LIBPT_ERR_NOMEM;
+        CK(slice_b_launch(d.src, d.P, (int)d.K, d.N, d.w, d.wsrc, d.ldsrc, kpi,
+                          std::ldexp(1.0, d.part ? k : 0), f->e, S, pl,
+                          p->st));
+      }
+      p->i8planes.push_back({key, pl});
+    }
+    int r = d.role == 0 ? i8_map_a(&c.tcmaps.m[i], pl, d.K, d.R, d.Q, d.P, S)
+                        : i8_map_b(&c.tcmaps.m[i], pl, d.K, d.N, d.P, S);
+    if (r) return r;
+  }
+  // each job's output rows / columns take the scales of its operand families
+  for (JobT &j : c.jobs) {
+    for (Family &f : p->fams) {
+      if (f.id == c.opd[j.seg[0].amap].fam) j.ea = f.e;
+      if (f.id == c.opd[j.seg[0].bmap].fam) j.eb = f.e;
+    }
+  }
+  return LIBPT_OK;
+}
+
 int add_cases(libpt_plan *p) {
   const int oa = p->oa, va = p->va, ob = p->ob, vb = p->vb;
   auto add = [&](int type, int flip, int o1, int v1, int o2, int v2) {
@@ -661,6 +898,13 @@ int add_cases(libpt_plan *p) {
     int r = c.type == 0 ? build_aaa(p, c) : build_aab(p, c);
     if (!r && p->precision == LIBPT_PREC_TF32X3) r = build_tc(p, c);
     if (r) return r;
+  }
+  if (p->precision == LIBPT_PREC_EMU64) {
+    if (int r = i8_maxima(p)) return r;
+    if (int r = i8_exponents(p)) return r;
+    for (SpinCase &c : p->cases)
+      if (c.count)
+        if (int r = i8_planes(p, c)) return r;
   }
   return LIBPT_OK;
 }
@@ -719,7 +963,11 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
         g.M = jt.M;
         g.N = jt.N;
         const bool tc = p->precision == LIBPT_PREC_TF32X3;
-        const int bn = tc ? TC_BN : GEMM_BN, bmr = tc ? TC_BM : c.bm;
+        const bool i8 = p->precision == LIBPT_PREC_EMU64;
+        const int bn = tc ? TC_BN : i8 ? TC_I8_BN : GEMM_BN;
+        const int bmr = (tc || i8) ? TC_BM : c.bm;
+        g.ea = jt.ea;
+        g.eb = jt.eb;
         g.ntiles_n = (jt.N + bn - 1) / bn;
         g.mtiles = (jt.M + bmr - 1) / bmr;
         g.tile_begin = tiles;
@@ -735,6 +983,8 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
           gs.b_p = ijk[st.bp];
           gs.ksteps = tc ? (st.k + tc_kchunk_elems(TC_TF32) - 1) /
                                tc_kchunk_elems(TC_TF32)
+                    : i8 ? (st.k + tc_kchunk_elems(TC_INT8) - 1) /
+                               tc_kchunk_elems(TC_INT8)
                          : st.ksteps;
         }
         tiles += g.mtiles * g.ntiles_n;
@@ -752,7 +1002,12 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
       for (int x = 0; x < 4; ++x) CK(cudaEventCreate(&ev[x]));
       CK(cudaEventRecord(ev[0], p->st));
     }
-    if (p->precision == LIBPT_PREC_TF32X3) {
+    if (p->precision == LIBPT_PREC_EMU64) {
+      TcProducts pr;
+      memset(&pr, 0, sizeof(pr));
+      CK(gemm_tc_launch(TC_INT8, c.tcmaps, p->d_jobs, (int)jobs.size(), tiles,
+                        pr, p->d_err, p->st, p->slices));
+    } else if (p->precision == LIBPT_PREC_TF32X3) {
       TcProducts pr;
       memset(&pr, 0, sizeof(pr));
       const int8_t pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};   // hh + hl + lh
@@ -811,8 +1066,16 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     set_error("libpt_plan_create: bad kind/dtype/args");
     return LIBPT_ERR_ARG;
   }
-  if (precision != LIBPT_PREC_FP64 && precision != LIBPT_PREC_TF32X3) {
+  int slices = (precision >> 8) & 0xFF;
+  precision &= 0xFF;
+  if (precision != LIBPT_PREC_FP64 && precision != LIBPT_PREC_TF32X3 &&
+      precision != LIBPT_PREC_EMU64) {
     set_error("libpt_plan_create: unknown precision mode");
+    return LIBPT_ERR_ARG;
+  }
+  if (slices == 0) slices = 6;
+  if (slices < TC_S_MIN || slices > TC_S_MAX) {
+    set_error("libpt_plan_create: emulated FP64 takes 4 to 7 slices");
     return LIBPT_ERR_ARG;
   }
   if (arena && precision != LIBPT_PREC_FP64) {
@@ -845,6 +1108,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
   p->vb = (int)vb;
   p->dtype = dtype;
   p->precision = precision;
+  p->slices = slices;
   p->st = st;
   p->factor = unr ? 1.0 : 2.0;   // src/pt.c:478, 534, 971, 1049
   p->arena = static_cast<char *>(arena);
@@ -889,8 +1153,8 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       break;
     }
     if ((r = add_cases(p))) break;
-    if (p->precision == LIBPT_PREC_TF32X3) {
-      // the tensor-core path reads planes; of the padded FP64 blocks only the
+    if (p->precision != LIBPT_PREC_FP64) {
+      // the tensor-core paths read planes; of the padded FP64 blocks only the
       // amplitudes stay (the energy epilogue's disconnected term reads them)
       if (cudaStreamSynchronize(st) != cudaSuccess) {
         set_error("preparing tensor-core planes failed");

@@ -28,11 +28,26 @@ struct OpDesc {
   int role = -1;    // 0: A, 1: B, -1: unused
   const double *src = nullptr;
   int64_t K = 0, R = 0, Q = 0, P = 0, N = 0, Nld = 0;
+  // B source geometry: element (p, k, n) at src[(p K + k) ldsrc + col(n)],
+  // col(n) = (n / w) wsrc + n % w, zero when n % w >= wsrc
+  int64_t ldsrc = 0, w = 0, wsrc = 0;
+  // emulated FP64: scale family (operands of one job side share row / column
+  // scales) and part (0: amplitude x OVVV product, 1: OOVO x amplitude)
+  int fam = -1, part = 0;
 };
 
 // TF32 hi/lo planes of one operand, in tensor-core layout.
 struct Planes {
   float *hi = nullptr, *lo = nullptr;
+};
+
+// Emulated-FP64 state of one scale family.
+struct Family {
+  int id = -1;
+  int64_t n = 0;                          // rows (A) or columns (B)
+  unsigned long long *max0 = nullptr;     // per row/column |max| of part 0
+  unsigned long long *max1 = nullptr;     // ... of part 1
+  signed char *e = nullptr;               // joint exponents
 };
 
 struct JobT {
@@ -41,6 +56,7 @@ struct JobT {
   int64_t ldc;
   int nseg;
   SegT seg[MAX_SEG];
+  const signed char *ea = nullptr, *eb = nullptr;   // emulated FP64 scales
 };
 
 // Padded device copies of one amplitude + integral set (index 0 aaaa,
@@ -50,6 +66,10 @@ struct OperandSet {
   double *taup[2] = {nullptr, nullptr};
   double *ovvv[4] = {nullptr, nullptr, nullptr, nullptr};
   double *oovo[4] = {nullptr, nullptr, nullptr, nullptr};
+  // emulated FP64 from device inputs: the caller's pt.h OVVV blocks are
+  // sliced in place (no padded FP64 copy); ovvv[] is then null
+  const double *ovvv_src[4] = {nullptr, nullptr, nullptr, nullptr};
+  int balance = 0;   // OOVO x amplitude products: A scaled 2^-balance, B 2^+
 };
 
 struct SpinCase {
@@ -102,6 +122,10 @@ struct libpt_plan {
   size_t arena_size = 0, arena_used = 0;
   // tensor-core planes, keyed by (source block, role)
   std::vector<std::pair<std::pair<const double *, int>, ptb::Planes>> planes;
+  // emulated FP64: digit planes per (source block, role), scale families
+  int slices = 6;
+  std::vector<std::pair<std::pair<const double *, int>, signed char *>> i8planes;
+  std::vector<ptb::Family> fams;
   // kernel timing (libpt_plan_timing): events around each launch
   bool timing = false;
   std::vector<cudaEvent_t> ev_gemm, ev_epi;  // start/stop pairs
@@ -125,6 +149,12 @@ size_t rpt_arena_bytes(int64_t o, int64_t v, int64_t nb);
 int tc_map_a(CUtensorMap *m, const float *p, int64_t K, int64_t R, int64_t Q,
              int64_t P);
 int tc_map_b(CUtensorMap *m, const float *p, int64_t K, int64_t N, int64_t P);
+// INT8 digit-plane views: A planes [2S][P][Q][R][kpi] as (K, R, Q, P, 2S),
+// B planes [S][P][N][kpi] as (K, N, P, S); kpi = K rounded up to 16.
+int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
+             int64_t Q, int64_t P, int S);
+int i8_map_b(CUtensorMap *m, const signed char *p, int64_t K, int64_t N,
+             int64_t P, int S);
 // DMMA views of padded FP64 blocks: A [P][Q][R][pad4(K)], B [P][K][Nld].
 int dmma_map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R,
                int64_t Q, int64_t P, int bm);

@@ -157,3 +157,204 @@ cudaError_t transpose_split_tf32_launch(const double *src, float *hi,
 }
 
 }  // namespace ptb
+
+// ---- emulated FP64: power-of-two scales and signed 7-bit digit planes ----
+//
+// An operand value a with scale exponent e is written as
+//   a * 2^-e = sum_{p=1..S} d_p 2^-7p (+ remainder < 2^-7S / 2),  |d_p| <= 64,
+// digits by round-to-nearest of the running remainder (Ozaki-style slicing;
+// all steps exact in FP64).  e is chosen per A row / B column as
+// ceil-log2(max |a|) + 1, so |a 2^-e| <= 1/2.
+
+namespace ptb {
+
+namespace {
+
+__device__ __forceinline__ void atomic_max_pos(unsigned long long *m,
+                                               double x) {
+  // non-negative doubles order like their bit patterns
+  atomicMax(m, (unsigned long long)__double_as_longlong(x));
+}
+
+// rmax[x] = max over (pq, k < K) |src[pq][x][k]|, src rows padded to kp.
+__global__ void rowmax_kernel(const double *__restrict__ src, int64_t npq,
+                              int64_t R, int64_t K, int64_t kp,
+                              unsigned long long *rmax) {
+  const int64_t rows = npq * R;
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 32;
+       r < rows; r += ((int64_t)gridDim.x * blockDim.x) / 32) {
+    double m = 0.0;
+    for (int64_t k = lane; k < K; k += 32) m = fmax(m, fabs(src[r * kp + k]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(~0u, m, o));
+    if (lane == 0 && m > 0.0) atomic_max_pos(&rmax[r % R], m);
+  }
+}
+
+// Column n of a B operand [P][K][N] whose N index is row-padded: n = y*w + c
+// with c < wsrc real (source offset y*wsrc + c) and c >= wsrc zero.
+__device__ __forceinline__ int64_t bsrc_col(int64_t n, int64_t w,
+                                            int64_t wsrc) {
+  const int64_t y = n / w, c = n - y * w;
+  return c < wsrc ? y * wsrc + c : -1;
+}
+
+// cmax[n] = max over (p, k) |B[p][k][n]|; source rows of length ldsrc.
+__global__ void colmax_kernel(const double *__restrict__ src, int64_t K,
+                              int64_t N, int64_t w, int64_t wsrc,
+                              int64_t ldsrc, unsigned long long *cmax) {
+  const int64_t p = blockIdx.y;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < N;
+       n += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = bsrc_col(n, w, wsrc);
+    if (c < 0) continue;
+    const double *s = src + p * K * ldsrc + c;
+    double m = 0.0;
+    for (int64_t k = 0; k < K; ++k) m = fmax(m, fabs(s[k * ldsrc]));
+    if (m > 0.0) atomic_max_pos(&cmax[n], m);
+  }
+}
+
+// e[x] = exponent with max(m1[x], m2[x] * s2) * 2^-e in [1/4, 1/2).
+__global__ void exps_kernel(const unsigned long long *m1,
+                            const unsigned long long *m2, double s2,
+                            int64_t n, signed char *e) {
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    double m = __longlong_as_double((long long)m1[x]);
+    if (m2) m = fmax(m, __longlong_as_double((long long)m2[x]) * s2);
+    int E = 0;
+    if (m > 0.0) frexp(m, &E);
+    E += 1;
+    e[x] = (signed char)(E < -120 ? -120 : E > 120 ? 120 : E);
+  }
+}
+
+__device__ __forceinline__ void digits(double s, int S, signed char *d) {
+  for (int q = 0; q < S; ++q) {
+    const double t = s * 128.0;
+    const double r = rint(t);
+    d[q] = (signed char)r;
+    s = t - r;
+  }
+}
+
+// A side: src[npq][R][kp] (FP64) -> out[2S][npq][R][kpi] int8: digit planes
+// of a * scale * 2^-ea[x], then their negatives.
+__global__ void slice_a_kernel(const double *__restrict__ src, int64_t npq,
+                               int64_t R, int64_t K, int64_t kp, int64_t kpi,
+                               double scale, const signed char *ea, int S,
+                               signed char *__restrict__ out) {
+  const int64_t n = npq * R * kpi, plane = n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / kpi, k = i - r * kpi;
+    const double a = k < K ? src[r * kp + k] : 0.0;
+    signed char d[8];
+    digits(ldexp(a * scale, -ea[r % R]), S, d);
+    for (int q = 0; q < S; ++q) {
+      out[q * plane + i] = d[q];
+      out[(S + q) * plane + i] = (signed char)(-d[q]);
+    }
+  }
+}
+
+// B side, transposed: B[P][K][N] (row-padded N, see bsrc_col) ->
+// out[S][P][N][kpi] int8 digit planes of b * scale * 2^-eb[n].
+__global__ void slice_b_kernel(const double *__restrict__ src, int K,
+                               int64_t N, int64_t w, int64_t wsrc,
+                               int64_t ldsrc, int64_t kpi, double scale,
+                               const signed char *eb, int S, int64_t P,
+                               signed char *__restrict__ out) {
+  __shared__ double t[32][33];
+  const int64_t p = blockIdx.z;
+  const int64_t n0 = (int64_t)blockIdx.x * 32;
+  const int k0 = blockIdx.y * 32;
+  const double *s = src + p * K * ldsrc;
+  for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+    const int k = k0 + rr;
+    const int64_t n = n0 + threadIdx.x;
+    const int64_t c = n < N ? bsrc_col(n, w, wsrc) : -1;
+    t[rr][threadIdx.x] = (k < K && c >= 0) ? s[(int64_t)k * ldsrc + c] : 0.0;
+  }
+  __syncthreads();
+  const int64_t plane = P * N * kpi;
+  for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+    const int64_t n = n0 + rr;
+    const int k = k0 + threadIdx.x;
+    if (n < N && k < kpi) {
+      signed char d[8];
+      digits(ldexp(t[threadIdx.x][rr] * scale, -eb[n]), S, d);
+      const int64_t o = (p * N + n) * kpi + k;
+      for (int q = 0; q < S; ++q) out[q * plane + o] = d[q];
+    }
+  }
+}
+
+int grid2(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  if (b > 148 * 32) b = 148 * 32;
+  return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+cudaError_t rowmax_launch(const double *src, int64_t npq, int64_t R, int64_t K,
+                          int64_t kp, unsigned long long *rmax,
+                          cudaStream_t st) {
+  if (npq * R <= 0 || K <= 0) return cudaSuccess;
+  rowmax_kernel<<<grid2(npq * R * 32), 256, 0, st>>>(src, npq, R, K, kp, rmax);
+  return cudaGetLastError();
+}
+
+cudaError_t colmax_launch(const double *src, int64_t P, int64_t K, int64_t N,
+                          int64_t w, int64_t wsrc, int64_t ldsrc,
+                          unsigned long long *cmax, cudaStream_t st) {
+  if (P <= 0 || K <= 0 || N <= 0) return cudaSuccess;
+  for (int64_t p0 = 0; p0 < P; p0 += 65535) {
+    const int64_t np_ = P - p0 < 65535 ? P - p0 : 65535;
+    dim3 grid((unsigned)((N + 255) / 256 < 1024 ? (N + 255) / 256 : 1024),
+              (unsigned)np_);
+    colmax_kernel<<<grid, 256, 0, st>>>(src + p0 * K * ldsrc, K, N, w, wsrc,
+                                        ldsrc, cmax);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t exps_launch(const unsigned long long *m1,
+                        const unsigned long long *m2, double s2, int64_t n,
+                        signed char *e, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  exps_kernel<<<grid2(n), 256, 0, st>>>(m1, m2, s2, n, e);
+  return cudaGetLastError();
+}
+
+cudaError_t slice_a_launch(const double *src, int64_t npq, int64_t R,
+                           int64_t K, int64_t kp, int64_t kpi, double scale,
+                           const signed char *ea, int S, signed char *out,
+                           cudaStream_t st) {
+  if (npq * R <= 0) return cudaSuccess;
+  slice_a_kernel<<<grid2(npq * R * kpi), 256, 0, st>>>(src, npq, R, K, kp, kpi,
+                                                       scale, ea, S, out);
+  return cudaGetLastError();
+}
+
+cudaError_t slice_b_launch(const double *src, int64_t P, int K, int64_t N,
+                           int64_t w, int64_t wsrc, int64_t ldsrc, int64_t kpi,
+                           double scale, const signed char *eb, int S,
+                           signed char *out, cudaStream_t st) {
+  if (P <= 0 || N <= 0 || kpi <= 0) return cudaSuccess;
+  for (int64_t p0 = 0; p0 < P; p0 += 65535) {
+    const int64_t np_ = P - p0 < 65535 ? P - p0 : 65535;
+    dim3 grid((unsigned)((N + 31) / 32), (unsigned)((kpi + 31) / 32),
+              (unsigned)np_);
+    // planes keep their full [P] extent: offset the output by p0 rows
+    slice_b_kernel<<<grid, dim3(32, 8), 0, st>>>(
+        src + p0 * K * ldsrc, K, N, w, wsrc, ldsrc, kpi, scale, eb, S, P,
+        out + p0 * N * kpi);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace ptb

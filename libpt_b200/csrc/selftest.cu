@@ -19,7 +19,7 @@ namespace {
 // Values exactly representable in FP32 (so the TF32 planes split them
 // exactly), uniform in (-1, 1), from an integer hash of (seed, index).
 __global__ void fill_kernel(double *x, int64_t rows, int64_t w, int64_t ld,
-                            uint32_t seed) {
+                            uint32_t seed, int full) {
   const int64_t n = rows * ld;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -31,7 +31,11 @@ __global__ void fill_kernel(double *x, int64_t rows, int64_t w, int64_t ld,
     h *= 0x846ca68bu;
     h ^= h >> 16;
     const float u = (float)(h >> 8) * (1.0f / 8388608.0f) - 1.0f;
-    x[i] = c < w ? (double)u : 0.0;
+    // full: add 29 more random bits below the FP32 value (FP64 operands)
+    const double lo = full ? (double)(h & 0xFFu) * 0x1p-32 +
+                                 (double)((i * 0x9E3779B97F4A7C15ull) >> 43) * 0x1p-53
+                           : 0.0;
+    x[i] = c < w ? (double)u + lo : 0.0;
   }
 }
 
@@ -47,14 +51,23 @@ __global__ void ref_kernel(const double *A, const double *B1, const double *B2,
   C[r * ldb + c] = s;
 }
 
+ptb::TcMapSet &tcmaps_scratch() {
+  static ptb::TcMapSet m;
+  return m;
+}
+
 }  // namespace
 
 LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
                              double *rel_err) {
   using namespace ptb;
+  int slices = (precision >> 8) & 0xFF;
+  precision &= 0xFF;
+  if (slices == 0) slices = 6;
   if (!rel_err || m < 1 || n < 1 || k < 1 || m > 4096 || n > 4096 ||
-      k > 4096 || (precision != LIBPT_PREC_FP64 &&
-                   precision != LIBPT_PREC_TF32X3)) {
+      k > 4096 || slices < TC_S_MIN || slices > TC_S_MAX ||
+      (precision != LIBPT_PREC_FP64 && precision != LIBPT_PREC_TF32X3 &&
+       precision != LIBPT_PREC_EMU64)) {
     set_error("libpt_selftest: bad arguments");
     return LIBPT_ERR_ARG;
   }
@@ -81,9 +94,10 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
     set_error("libpt_selftest: cudaMalloc failed");
     return done(LIBPT_ERR_NOMEM);
   }
-  fill_kernel<<<256, 256>>>(A, m, k, kp, 1);
-  fill_kernel<<<256, 256>>>(B1, k, n, np, 2);
-  fill_kernel<<<256, 256>>>(B2, k, n, np, 3);
+  const int full = precision == LIBPT_PREC_EMU64;
+  fill_kernel<<<256, 256>>>(A, m, k, kp, 1, full);
+  fill_kernel<<<256, 256>>>(B1, k, n, np, 2, full);
+  fill_kernel<<<256, 256>>>(B2, k, n, np, 3, full);
   cudaMemset(Cm, 0, (size_t)m * np * 8);
   cudaMemset(err, 0, 4);
   ref_kernel<<<(unsigned)(((int64_t)m * n + 255) / 256), 256>>>(A, B1, B2, Cr, m,
@@ -115,6 +129,58 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
     cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
     ce = gemm_dmma_launch(maps, dj, 1, job.mtiles * job.ntiles_n, 128, err,
                           nullptr);
+  } else if (precision == LIBPT_PREC_EMU64) {
+    // one A family (A itself) and one B family (B1 part 0, B2 part 1)
+    const int S = slices;
+    const int64_t kpi = (k + 15) & ~int64_t(15);
+    unsigned long long *ma = (unsigned long long *)alloc((size_t)m * 8 + 8);
+    unsigned long long *mb0 = (unsigned long long *)alloc((size_t)np * 8 + 8);
+    unsigned long long *mb1 = (unsigned long long *)alloc((size_t)np * 8 + 8);
+    signed char *ea = (signed char *)alloc((size_t)m + 16);
+    signed char *eb = (signed char *)alloc((size_t)np + 16);
+    signed char *pa = (signed char *)alloc((size_t)2 * S * m * kpi);
+    signed char *pb1 = (signed char *)alloc((size_t)S * np * kpi);
+    signed char *pb2 = (signed char *)alloc((size_t)S * np * kpi);
+    if (!ma || !mb0 || !mb1 || !ea || !eb || !pa || !pb1 || !pb2) {
+      set_error("libpt_selftest: cudaMalloc failed");
+      return done(LIBPT_ERR_NOMEM);
+    }
+    cudaMemset(ma, 0, (size_t)m * 8 + 8);
+    cudaMemset(mb0, 0, (size_t)np * 8 + 8);
+    cudaMemset(mb1, 0, (size_t)np * 8 + 8);
+    if ((ce = rowmax_launch(A, 1, m, k, kp, ma, nullptr)) ||
+        (ce = colmax_launch(B1, 1, k, np, np, np, np, mb0, nullptr)) ||
+        (ce = colmax_launch(B2, 1, k, np, np, np, np, mb1, nullptr)) ||
+        (ce = exps_launch(ma, nullptr, 1.0, m, ea, nullptr)) ||
+        (ce = exps_launch(mb0, mb1, 1.0, np, eb, nullptr)) ||
+        (ce = slice_a_launch(A, 1, m, k, kp, kpi, 1.0, ea, S, pa, nullptr)) ||
+        (ce = slice_b_launch(B1, 1, k, np, np, np, np, kpi, 1.0, eb, S, pb1,
+                             nullptr)) ||
+        (ce = slice_b_launch(B2, 1, k, np, np, np, np, kpi, 1.0, eb, S, pb2,
+                             nullptr))) {
+      set_error(cudaGetErrorString(ce));
+      return done(LIBPT_ERR_CUDA);
+    }
+    if ((r = i8_map_a(&(tcmaps_scratch().m[0]), pa, k, m, 1, 1, S)) ||
+        (r = i8_map_b(&(tcmaps_scratch().m[1]), pb1, k, np, 1, S)) ||
+        (r = i8_map_b(&(tcmaps_scratch().m[2]), pb2, k, np, 1, S)))
+      return done(r);
+    job.mtiles = (m + TC_BM - 1) / TC_BM;
+    job.ntiles_n = (int)((np + TC_I8_BN - 1) / TC_I8_BN);
+    job.ea = ea;
+    job.eb = eb;
+    const int kc = tc_kchunk_elems(TC_INT8);
+    for (int s2 = 0; s2 < 2; ++s2) {
+      job.seg[s2].amap = 0;
+      job.seg[s2].bmap = (int16_t)(1 + s2);
+      job.seg[s2].neg = (int16_t)s2;
+      job.seg[s2].ksteps = (k + kc - 1) / kc;
+    }
+    TcProducts pr;
+    memset(&pr, 0, sizeof(pr));
+    cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
+    ce = gemm_tc_launch(TC_INT8, tcmaps_scratch(), dj, 1,
+                        job.mtiles * job.ntiles_n, pr, err, nullptr, S);
   } else {
     float *pl[6];
     for (int x = 0; x < 6; ++x) {

@@ -22,6 +22,7 @@ ERRORS = {1: "LIBPT_ERR_ARG", 2: "LIBPT_ERR_NOMEM", 3: "LIBPT_ERR_CUDA",
           4: "LIBPT_ERR_TIMEOUT", 5: "LIBPT_ERR_UNSUPPORTED"}
 PREC_FP64 = 0
 PREC_TF32X3 = 1
+PREC_EMU64 = 2          # | (slices << 8), slices 4..7 (default 6)
 
 _lib = None
 

@@ -167,3 +167,29 @@ def test_synthetic_tf32x3_plan(kind, sz):
     e = p.energy()
     p.close()
     assert abs(e - ref) <= 2e-5 * abs(ref)
+
+
+@pytest.mark.parametrize("name", fixtures.NAMES)
+def test_golden_emulated_fp64(name, energies):
+    """Emulated FP64 (6 slices) on the golden fixtures: the reference FP64
+    value to 1e-12 Eh (measured <= 1e-14)."""
+    case = fixtures.load(name)
+    p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64)
+    p.run()
+    e = p.energy()
+    p.close()
+    assert abs(e - energies[name]["ref_fp64"]) <= 1e-12
+
+
+@pytest.mark.parametrize("kind,sz", [("rpt", (8, 64)), ("upt", (5, 21, 4, 23)),
+                                     ("rft", (5, 30)), ("uft", (4, 17, 3, 19))])
+def test_synthetic_emulated_fp64(kind, sz):
+    """Stated tolerance of emulated FP64 (6 slices): |dE| <= 1e-6 Eh and
+    <= 1e-12 |E| against the reference FP64 (measured <= 9e-12 Eh)."""
+    case = synth.make(kind, *sz, seed=5, fock=1e-3)
+    ref = oracle.solve(checker(), case)
+    p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64)
+    p.run()
+    e = p.energy()
+    p.close()
+    assert abs(e - ref) <= 1e-6 and abs(e - ref) <= 1e-12 * abs(ref)
