@@ -115,9 +115,17 @@ const char *libpt_last_error(void);
 
 /* Built-in self-test of a contraction kernel: C = A B1 - A B2 on random
  * m x k and k x n operands, against an FP64 reference computed on the device;
- * writes max|C - C_ref| / max|C_ref| to *rel_err.  precision selects the
- * kernel (LIBPT_PREC_*).  No counterpart in the reference. */
+ * writes max|C - C_ref| / max(|A| (|B1| + |B2|)) to *rel_err (the error over
+ * the scale that bounds a dot product's rounding).  precision selects the
+ * kernel (LIBPT_PREC_*, with the slice count in bits 8-15 for
+ * LIBPT_PREC_EMU64) and bits 16-23 a tile variant: FP64 0 = 128-row,
+ * 1 = 96-row tiles; emulated FP64 the index of one of the slice count's
+ * INT8 tile shapes (0 = widest); libpt_selftest_variants() counts them.
+ * No counterpart in the reference. */
 int libpt_selftest(int precision, int m, int n, int k, double *rel_err);
+/* Number of tile variants libpt_selftest accepts for a precision (with its
+ * slice count in bits 8-15).  No counterpart in the reference. */
+int libpt_selftest_variants(int precision);
 
 /* ---- device-pointer twins ----------------------------------------------
  * Same arguments as the reference entry points, but every tensor is a

@@ -24,9 +24,9 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
          "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 HOST_CXX = "/usr/bin/g++"   # the image's $CXX wrapper lacks some runtime specs
 
-SOURCES = ["gemm_dmma.cu", "gemm_tc.cu", "epilogue.cu", "prep.cu", "plan.cu", "api.cpp",
-           "noalloc.cu", "selftest.cu"]
-HEADERS = ["common.cuh", "engine.h", "plan.h"]
+SOURCES = ["gemm_dmma.cu", "gemm_tc.cu", "gemm_i8.cu", "epilogue.cu", "prep.cu",
+           "plan.cu", "tune.cpp", "api.cpp", "noalloc.cu", "selftest.cu"]
+HEADERS = ["common.cuh", "engine.h", "plan.h", "tune.h"]
 
 
 def _newer(target, deps):

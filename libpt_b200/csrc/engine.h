@@ -67,9 +67,6 @@ constexpr int TC_BM = 128;    // rows of a tile (TMEM lanes)
 constexpr int TC_BN = 256;    // columns of a tile
 constexpr int TC_TF32 = 0;    // kinds
 constexpr int TC_INT8 = 1;
-// Emulated FP64: S digit planes per operand, products with p + q <= S - 1
-// (0-based) into S accumulators of TC_I8_BN columns (single buffered).
-constexpr int TC_I8_BN = 64;
 constexpr int TC_S_MIN = 4, TC_S_MAX = 7;
 constexpr int TC_MAX_MAPS = 48;
 
@@ -82,14 +79,30 @@ struct TcProducts {           // acc[c] += A_plane[pa] * B_plane[pb]^T
   int n;
 };
 
-int tc_kchunk_elems(int kind);   // K elements per pipeline stage
-// kind TC_TF32: planes {hi, lo} in separate maps (2i, 2i+1), products from
-// prods.  kind TC_INT8: `slices` digit planes as a coordinate of one map per
-// operand (A maps hold 2*slices planes: the digits, then their negatives).
+int tc_kchunk_elems(int kind);   // K elements per pipeline stage (TF32)
+// 3xTF32: planes {hi, lo} in separate maps (2i, 2i+1), products from prods.
 cudaError_t gemm_tc_launch(int kind, const TcMapSet &maps,
                            const GemmJob *d_jobs, int njobs, int total_tiles,
                            const TcProducts &prods, unsigned *d_err,
                            cudaStream_t st, int slices = 0);
+
+// ---- emulated FP64 (tcgen05 kind::i8, gemm_i8.cu) ---------------------------
+//
+// S digit planes per operand, the products with p + q <= S - 1 (0-based)
+// into S INT32 accumulators of bn columns.  The digit planes are a
+// coordinate of one map per operand: A maps [2S][P][Q][R][kpi] hold the
+// digits then their negatives, B maps [S][P][N][kpi]; both viewed with
+// boxes of kc bytes x (128 | bn) rows, swizzled to kc bytes.
+struct I8Tile {
+  int bn;   // tile columns (multiple of 16, S * bn <= 512)
+  int kc;   // K bytes per pipeline stage (32 or 64)
+};
+// The tile variants compiled for a slice count (widest first); returns
+// their number (0 for an unsupported count).
+int i8_tiles(int slices, const I8Tile **out);
+cudaError_t gemm_i8_launch(int slices, I8Tile tile, const TcMapSet &maps,
+                           const GemmJob *d_jobs, int njobs, int total_tiles,
+                           unsigned *d_err, cudaStream_t st);
 
 // ---- energy epilogues ------------------------------------------------------
 

@@ -1,20 +1,13 @@
-// Tensor-core (tcgen05) contraction kernel for the multi-segment jobs.
+// Tensor-core (tcgen05) contraction kernel for the multi-segment jobs, in
+// 3xTF32 form (FP32-level accuracy).
 //
 // Same job/segment structure as gemm_dmma.cu (one triple's contraction
 // output = sum of signed amplitude x integral products), but the products
 // run on the 5th-generation tensor cores with accumulators in TMEM.  Each
-// operand is stored as NPL "planes", and a tile's result is assembled from
-// plane products accumulated in TMEM:
-//
-//  * TF32 (3xTF32, FP32-level): planes {hi, lo} of FP32 values, products
-//    hi*hi + hi*lo + lo*hi into one FP32 accumulator; the MMA's negate bit
-//    applies a segment's sign.
-//  * INT8 (emulated FP64, Ozaki-style): planes = S signed 7-bit digits of
-//    the operand scaled by a power of two per row (A) / column (B); the
-//    products d^A_p d^B_q with p + q <= S-1 are summed exactly in INT32, one
-//    accumulator per digit weight 2^-7(p+q+2), and the epilogue forms
-//       C = 2^(ea[row] + eb[col]) * sum_w acc_w 2^-7(w+2)        in FP64.
-//    Subtracted segments read the negated digit planes (A planes S..2S-1).
+// operand is stored as planes {hi, lo} of its FP32 values, and a tile's
+// result is hi*hi + hi*lo + lo*hi accumulated in one FP32 TMEM accumulator;
+// the MMA's negate bit applies a segment's sign.  (The emulated-FP64 INT8
+// kernel is gemm_i8.cu.)
 //
 // Warp roles (persistent CTA, one per SM):
 //   warp 0      TMA producer: A and B plane tiles of one K chunk per stage
@@ -22,8 +15,8 @@
 //   warp 1      TMEM owner and MMA issuer: one thread issues tcgen05.mma for
 //               every product and K step; tcgen05.commit frees the stage
 //   warps 2-5   epilogue: tcgen05.ld of the finished accumulators, FP64
-//               store (TF32: accumulators double buffered in TMEM so the
-//               next tile's MMAs overlap the drain)
+//               store (accumulators double buffered in TMEM so the next
+//               tile's MMAs overlap the drain)
 // All mbarrier waits are bounded; on expiry the kernel records the error,
 // stops issuing, still releases TMEM, and returns.
 #include "common.cuh"
@@ -68,18 +61,12 @@ __device__ __forceinline__ void tc_fence_after() {
 template <int KIND>
 __device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db,
                                        uint32_t idesc, uint32_t accum) {
-  if (KIND == TC_TF32)
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(
-            tmem),
-        "l"(da), "l"(db), "r"(idesc), "r"(accum));
-  else
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(
-            tmem),
-        "l"(da), "l"(db), "r"(idesc), "r"(accum));
+  static_assert(KIND == TC_TF32, "TF32 operands");
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+          tmem),
+      "l"(da), "l"(db), "r"(idesc), "r"(accum));
 }
 
 __device__ __forceinline__ void tc_commit(uint64_t *bar) {
@@ -106,12 +93,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
       : "r"(taddr));
 }
 
-// Instruction descriptor: M = 128, N = BN, K-major A and B; TF32 inputs with
-// FP32 accumulation, or signed INT8 inputs with INT32 accumulation.
+// Instruction descriptor: M = 128, N = BN, K-major TF32 A and B with FP32
+// accumulation.
 template <int KIND, int BN>
 __host__ __device__ constexpr uint32_t tc_idesc() {
-  return (KIND == TC_TF32 ? ((1u << 4) | (2u << 7) | (2u << 10))
-                          : ((2u << 4) | (1u << 7) | (1u << 10))) |
+  static_assert(KIND == TC_TF32, "TF32 operands, FP32 accumulation");
+  return ((1u << 4) | (2u << 7) | (2u << 10)) |
          ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
@@ -125,7 +112,7 @@ struct TcCfg {
   static constexpr int B_TILE = BN * SW;          // bytes per B plane tile
   static constexpr int STAGE = NPL * (A_TILE + B_TILE);
   static constexpr int KSTEP = 32;                // bytes of K per MMA
-  static constexpr int KELEM = KIND == TC_TF32 ? SW / 4 : SW;
+  static constexpr int KELEM = SW / 4;            // TF32 elements per row
   static constexpr int TMEM_COLS = pow2_cols(NBUF * NACC * BN);
   static constexpr int SMEM = ST * STAGE + 1024 /*align*/ + 256 /*barriers*/;
   static_assert(NBUF * NACC * BN <= 512, "TMEM holds 512 columns");
@@ -194,18 +181,10 @@ __global__ void __launch_bounds__(192, 1)
           const int k0 = ks * C::KELEM;
 #pragma unroll
           for (int p = 0; p < NPL; ++p) {
-            if (KIND == TC_TF32) {
-              tma_load_4d(st_base + p * C::A_TILE, &maps.m[sg.amap + p],
-                          &full[stage], k0, m0, sg.a_q, sg.a_p);
-              tma_load_3d(st_base + NPL * C::A_TILE + p * C::B_TILE,
-                          &maps.m[sg.bmap + p], &full[stage], k0, n0, sg.b_p);
-            } else {
-              tma_load_5d(st_base + p * C::A_TILE, &maps.m[sg.amap],
-                          &full[stage], k0, m0, sg.a_q, sg.a_p,
-                          p + (sg.neg ? NPL : 0));
-              tma_load_4d(st_base + NPL * C::A_TILE + p * C::B_TILE,
-                          &maps.m[sg.bmap], &full[stage], k0, n0, sg.b_p, p);
-            }
+            tma_load_4d(st_base + p * C::A_TILE, &maps.m[sg.amap + p],
+                        &full[stage], k0, m0, sg.a_q, sg.a_p);
+            tma_load_3d(st_base + NPL * C::A_TILE + p * C::B_TILE,
+                        &maps.m[sg.bmap + p], &full[stage], k0, n0, sg.b_p);
           }
           if (++stage == ST) {
             stage = 0;
@@ -235,7 +214,7 @@ __global__ void __launch_bounds__(192, 1)
       uint32_t started = 0;   // bit c: accumulator c has been written
       for (int s = 0; s < job.nseg && ok; ++s) {
         const GemmSeg sg = job.seg[s];
-        const uint32_t neg = (KIND == TC_TF32 && sg.neg) ? (1u << 13) : 0u;
+        const uint32_t neg = sg.neg ? (1u << 13) : 0u;   // negate A
         for (int ks = 0; ks < sg.ksteps; ++ks) {
           if (!mbar_wait(&full[stage], phase, err)) {
             ok = false;
@@ -244,38 +223,18 @@ __global__ void __launch_bounds__(192, 1)
           tc_fence_after();
           const uint32_t sa = smem_u32(smem + stage * C::STAGE);
           const uint32_t sb = sa + NPL * C::A_TILE;
-          if (KIND == TC_TF32) {
-            for (int q = 0; q < prods.n; ++q) {
-              const int c = prods.acc[q];
-              const uint64_t da = kmajor_desc<SW>(sa + prods.pa[q] * C::A_TILE);
-              const uint64_t db = kmajor_desc<SW>(sb + prods.pb[q] * C::B_TILE);
+          for (int q = 0; q < prods.n; ++q) {
+            const int c = prods.acc[q];
+            const uint64_t da = kmajor_desc<SW>(sa + prods.pa[q] * C::A_TILE);
+            const uint64_t db = kmajor_desc<SW>(sb + prods.pb[q] * C::B_TILE);
 #pragma unroll
-              for (int kk = 0; kk < SW / C::KSTEP; ++kk) {
-                // 32-byte K steps through the swizzled row (K-major layout)
-                tc_mma<KIND>(acc0 + (uint32_t)(c * BN),
-                             da + (uint64_t)(kk * C::KSTEP >> 4),
-                             db + (uint64_t)(kk * C::KSTEP >> 4),
-                             tc_idesc<KIND, BN>() | neg, (started >> c) & 1u);
-                started |= 1u << c;
-              }
-            }
-          } else {
-#pragma unroll
-            for (int pa = 0; pa < NPL; ++pa) {
-              const uint64_t da = kmajor_desc<SW>(sa + pa * C::A_TILE);
-#pragma unroll
-              for (int pb = 0; pb + pa < NPL; ++pb) {
-                const int c = pa + pb;     // digit weight 2^-7(c+2)
-                const uint64_t db = kmajor_desc<SW>(sb + pb * C::B_TILE);
-#pragma unroll
-                for (int kk = 0; kk < SW / C::KSTEP; ++kk) {
-                  tc_mma<KIND>(acc0 + (uint32_t)(c * BN),
-                               da + (uint64_t)(kk * C::KSTEP >> 4),
-                               db + (uint64_t)(kk * C::KSTEP >> 4),
-                               tc_idesc<KIND, BN>(), (started >> c) & 1u);
-                  started |= 1u << c;
-                }
-              }
+            for (int kk = 0; kk < SW / C::KSTEP; ++kk) {
+              // 32-byte K steps through the swizzled row (K-major layout)
+              tc_mma<KIND>(acc0 + (uint32_t)(c * BN),
+                           da + (uint64_t)(kk * C::KSTEP >> 4),
+                           db + (uint64_t)(kk * C::KSTEP >> 4),
+                           tc_idesc<KIND, BN>() | neg, (started >> c) & 1u);
+              started |= 1u << c;
             }
           }
           tc_commit(&empty[stage]);   // stage reusable once these MMAs finish
@@ -303,43 +262,23 @@ __global__ void __launch_bounds__(192, 1)
       tc_fence_after();
       const int row = m0 + 32 * q + lane;
       double *orow = job.out + (int64_t)row * job.ldc;
-      const int erow = (KIND == TC_INT8 && row < job.M) ? job.ea[row] : 0;
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) +
                              (uint32_t)(ab * NACC * BN);
 #pragma unroll 1
       for (int c0 = 0; c0 < BN; c0 += 32) {
         double v[32];
         uint32_t r[32];
-        if (KIND == TC_TF32) {
-          tmem_ld32(tbase + c0, r);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        tmem_ld32(tbase + c0, r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-          for (int x = 0; x < 32; ++x) v[x] = (double)__uint_as_float(r[x]);
-        } else {
-          // exact integers scaled by powers of two, summed from the smallest
-          // digit weight up
-#pragma unroll
-          for (int x = 0; x < 32; ++x) v[x] = 0.0;
-#pragma unroll 1
-          for (int a = NACC - 1; a >= 0; --a) {
-            tmem_ld32(tbase + a * BN + c0, r);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int x = 0; x < 32; ++x)
-              v[x] += ldexp((double)(int)r[x], -7 * (a + 2));
-          }
-        }
+        for (int x = 0; x < 32; ++x) v[x] = (double)__uint_as_float(r[x]);
         if (row < job.M) {
 #pragma unroll
           for (int x = 0; x < 32; x += 2) {
             const int col = n0 + c0 + x;
             if (col < job.N) {
-              double v0 = v[x], v1 = v[x + 1];
-              if (KIND == TC_INT8) {
-                v0 = ldexp(v0, erow + job.eb[col]);
-                v1 = ldexp(v1, erow + job.eb[col + 1]);
-              }
-              *reinterpret_cast<double2 *>(orow + col) = make_double2(v0, v1);
+              *reinterpret_cast<double2 *>(orow + col) =
+                  make_double2(v[x], v[x + 1]);
             }
           }
         }
@@ -378,38 +317,19 @@ cudaError_t launch(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
   return cudaGetLastError();
 }
 
-// Emulated FP64 with S digit planes: 64-byte K chunks, stages as many as fit.
-template <int S>
-cudaError_t launch_i8(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
-                      int total_tiles, const TcProducts &prods,
-                      unsigned *d_err, cudaStream_t st) {
-  constexpr int STAGE = S * (TC_BM + TC_I8_BN) * 64;
-  constexpr int NST = (227 * 1024 - 1024 - 256) / STAGE;
-  static_assert(NST >= 2, "two pipeline stages at least");
-  return launch<TC_INT8, TC_I8_BN, S, S, (NST > 4 ? 4 : NST), 64, 1>(
-      maps, d_jobs, njobs, total_tiles, prods, d_err, st);
-}
-
 }  // namespace
 
-int tc_kchunk_elems(int kind) { return kind == TC_TF32 ? 32 : 64; }
+int tc_kchunk_elems(int kind) { return kind == TC_TF32 ? 32 : 0; }
 
 cudaError_t gemm_tc_launch(int kind, const TcMapSet &maps,
                            const GemmJob *d_jobs, int njobs, int total_tiles,
                            const TcProducts &prods, unsigned *d_err,
                            cudaStream_t st, int slices) {
+  (void)slices;
   if (total_tiles <= 0) return cudaSuccess;
-  if (kind == TC_TF32)
-    return launch<TC_TF32, TC_BN, 2, 1, 2, 128, 2>(maps, d_jobs, njobs,
-                                                   total_tiles, prods, d_err,
-                                                   st);
-  switch (slices) {
-    case 4: return launch_i8<4>(maps, d_jobs, njobs, total_tiles, prods, d_err, st);
-    case 5: return launch_i8<5>(maps, d_jobs, njobs, total_tiles, prods, d_err, st);
-    case 6: return launch_i8<6>(maps, d_jobs, njobs, total_tiles, prods, d_err, st);
-    case 7: return launch_i8<7>(maps, d_jobs, njobs, total_tiles, prods, d_err, st);
-    default: return cudaErrorInvalidValue;
-  }
+  if (kind != TC_TF32) return cudaErrorInvalidValue;
+  return launch<TC_TF32, TC_BN, 2, 1, 2, 128, 2>(maps, d_jobs, njobs,
+                                                 total_tiles, prods, d_err, st);
 }
 
 }  // namespace ptb

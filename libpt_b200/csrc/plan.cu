@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "plan.h"
+#include "tune.h"
 #include "pt.h"
 
 namespace ptb {
@@ -145,7 +146,7 @@ int dalloc(libpt_plan *p, void **ptr, size_t bytes);
 }  // namespace
 
 int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
-             int64_t Q, int64_t P, int S) {
+             int64_t Q, int64_t P, int S, int kc) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -156,11 +157,12 @@ int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
                         (cuuint64_t)P, (cuuint64_t)(2 * S)};
   cuuint64_t str[4] = {(cuuint64_t)kpi, (cuuint64_t)(R * kpi),
                        (cuuint64_t)(Q * R * kpi), (cuuint64_t)(P * Q * R * kpi)};
-  cuuint32_t box[5] = {64, (cuuint32_t)TC_BM, 1, 1, 1};
+  cuuint32_t box[5] = {(cuuint32_t)kc, (cuuint32_t)TC_BM, 1, 1, 1};
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, (void *)p, dims, str,
                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   kc == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled (INT8 A view) failed: " +
@@ -171,7 +173,7 @@ int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
 }
 
 int i8_map_b(CUtensorMap *m, const signed char *p, int64_t K, int64_t N,
-             int64_t P, int S) {
+             int64_t P, int S, int kc, int bn) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -182,11 +184,12 @@ int i8_map_b(CUtensorMap *m, const signed char *p, int64_t K, int64_t N,
                         (cuuint64_t)S};
   cuuint64_t str[3] = {(cuuint64_t)kpi, (cuuint64_t)(N * kpi),
                        (cuuint64_t)(P * N * kpi)};
-  cuuint32_t box[4] = {64, (cuuint32_t)TC_I8_BN, 1, 1};
+  cuuint32_t box[4] = {(cuuint32_t)kc, (cuuint32_t)bn, 1, 1};
   cuuint32_t es[4] = {1, 1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, (void *)p, dims, str,
                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   kc == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled (INT8 B view) failed: " +
@@ -808,6 +811,22 @@ int i8_exponents(libpt_plan *p) {
 }
 
 // Phase 4: digit planes of every operand and the INT8 tensor-core views.
+// Tensor maps of a case's digit planes for the plan's current tile variant.
+int i8_encode(libpt_plan *p, SpinCase &c) {
+  for (int i = 0; i < MAX_MAPS; ++i) {
+    const OpDesc &d = c.opd[i];
+    if (d.role < 0) continue;
+    const int r =
+        d.role == 0
+            ? i8_map_a(&c.tcmaps.m[i], c.i8pl[i], d.K, d.R, d.Q, d.P,
+                       p->slices, p->i8tile.kc)
+            : i8_map_b(&c.tcmaps.m[i], c.i8pl[i], d.K, d.N, d.P, p->slices,
+                       p->i8tile.kc, p->i8tile.bn);
+    if (r) return r;
+  }
+  return LIBPT_OK;
+}
+
 int i8_planes(libpt_plan *p, SpinCase &c) {
   const int S = p->slices;
   for (int i = 0; i < MAX_MAPS; ++i) {
@@ -838,10 +857,9 @@ int i8_planes(libpt_plan *p, SpinCase &c) {
       }
       p->i8planes.push_back({key, pl});
     }
-    int r = d.role == 0 ? i8_map_a(&c.tcmaps.m[i], pl, d.K, d.R, d.Q, d.P, S)
-                        : i8_map_b(&c.tcmaps.m[i], pl, d.K, d.N, d.P, S);
-    if (r) return r;
+    c.i8pl[i] = pl;
   }
+  if (int r = i8_encode(p, c)) return r;
   // each job's output rows / columns take the scales of its operand families
   for (JobT &j : c.jobs) {
     for (Family &f : p->fams) {
@@ -964,7 +982,7 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
         g.N = jt.N;
         const bool tc = p->precision == LIBPT_PREC_TF32X3;
         const bool i8 = p->precision == LIBPT_PREC_EMU64;
-        const int bn = tc ? TC_BN : i8 ? TC_I8_BN : GEMM_BN;
+        const int bn = tc ? TC_BN : i8 ? p->i8tile.bn : GEMM_BN;
         const int bmr = (tc || i8) ? TC_BM : c.bm;
         g.ea = jt.ea;
         g.eb = jt.eb;
@@ -983,8 +1001,7 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
           gs.b_p = ijk[st.bp];
           gs.ksteps = tc ? (st.k + tc_kchunk_elems(TC_TF32) - 1) /
                                tc_kchunk_elems(TC_TF32)
-                    : i8 ? (st.k + tc_kchunk_elems(TC_INT8) - 1) /
-                               tc_kchunk_elems(TC_INT8)
+                    : i8 ? (st.k + p->i8tile.kc - 1) / p->i8tile.kc
                          : st.ksteps;
         }
         tiles += g.mtiles * g.ntiles_n;
@@ -1003,10 +1020,8 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
       CK(cudaEventRecord(ev[0], p->st));
     }
     if (p->precision == LIBPT_PREC_EMU64) {
-      TcProducts pr;
-      memset(&pr, 0, sizeof(pr));
-      CK(gemm_tc_launch(TC_INT8, c.tcmaps, p->d_jobs, (int)jobs.size(), tiles,
-                        pr, p->d_err, p->st, p->slices));
+      CK(gemm_i8_launch(p->slices, p->i8tile, c.tcmaps, p->d_jobs,
+                        (int)jobs.size(), tiles, p->d_err, p->st));
     } else if (p->precision == LIBPT_PREC_TF32X3) {
       TcProducts pr;
       memset(&pr, 0, sizeof(pr));
@@ -1052,6 +1067,143 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
     CK(reduce_partials_launch(p->partials, c.ntiles, (int)n, p->d_slot,
                               p->e_slot, p->st));
   }
+  return LIBPT_OK;
+}
+
+// Device time of one run of `ents` (of case c), in milliseconds.
+int probe_ms(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents,
+             float *ms) {
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int r = LIBPT_OK;
+  CK(cudaEventRecord(e0, p->st));
+  r = run_case(p, c, ents);
+  if (!r) {
+    CK(cudaEventRecord(e1, p->st));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return r;
+}
+
+// Re-encodes a case's DMMA A views for CTA tile rows bm.
+int set_bm(SpinCase &c, int bm) {
+  c.bm = bm;
+  for (int i = 0; i < MAX_MAPS; ++i) {
+    const OpDesc &d = c.opd[i];
+    if (d.role == 0)
+      if (int r = map_a(&c.maps.m[i], d.src, d.K, d.R, d.Q, d.P, bm)) return r;
+  }
+  return LIBPT_OK;
+}
+
+// The autotuner: picks the kernel variants of a plan by timing them on a
+// probe of its triples (each candidate run twice, the second run timed),
+// and remembers the choice per (kind, sizes, precision, slices, dtype).
+//   FP64 DMMA:      CTA tile rows 96 or 128, per spin case
+//   emulated FP64:  the INT8 tile variants of the slice count (i8_tiles)
+// The probe's energies are discarded (slots reset afterwards); choices do
+// not change results, only speed (each output element is accumulated in
+// the same order by every variant).
+int autotune(libpt_plan *p) {
+  if (p->queue.empty() || p->precision == LIBPT_PREC_TF32X3) return LIBPT_OK;
+  const bool emu = p->precision == LIBPT_PREC_EMU64;
+  const std::string key = tune_key(p->kind, p->oa, p->va, p->ob, p->vb,
+                                   p->precision, emu ? p->slices : 0, p->dtype);
+  const I8Tile *tiles = nullptr;
+  const int ntiles = emu ? i8_tiles(p->slices, &tiles) : 0;
+  std::vector<int> choice;
+  if (tune_lookup(key, &choice)) {
+    if (emu && !choice.empty() && choice[0] >= 0 && choice[0] < ntiles) {
+      p->i8tile = tiles[choice[0]];
+      for (SpinCase &c : p->cases)
+        if (c.count)
+          if (int r = i8_encode(p, c)) return r;
+    } else if (!emu && choice.size() == p->cases.size()) {
+      for (size_t ci = 0; ci < p->cases.size(); ++ci)
+        if (p->cases[ci].count && (choice[ci] == 96 || choice[ci] == 128))
+          if (int r = set_bm(p->cases[ci], choice[ci])) return r;
+    }
+    return LIBPT_OK;
+  }
+  if (!tune_enabled()) return LIBPT_OK;
+  // probe: the first triples of the case with the most work
+  auto probe_of = [&](const SpinCase &c) {
+    const int64_t n = std::min<int64_t>(c.count, 4);
+    std::vector<int64_t> e((size_t)n);
+    for (int64_t x = 0; x < n; ++x) e[(size_t)x] = c.first + x;
+    return e;
+  };
+  int r = LIBPT_OK;
+  if (emu) {
+    size_t big = 0;
+    double most = -1.0;
+    for (size_t ci = 0; ci < p->cases.size(); ++ci) {
+      const SpinCase &c = p->cases[ci];
+      const double w = (double)c.count * c.flops_per_triple;
+      if (c.count && w > most) {
+        most = w;
+        big = ci;
+      }
+    }
+    const std::vector<int64_t> ents = probe_of(p->cases[big]);
+    int best = 0;
+    float best_ms = 0.f;
+    for (int t = 0; t < ntiles && !r; ++t) {
+      p->i8tile = tiles[t];
+      r = i8_encode(p, p->cases[big]);
+      float ms = 0.f;
+      if (!r) r = probe_ms(p, p->cases[big], ents, &ms);
+      if (!r) r = probe_ms(p, p->cases[big], ents, &ms);
+      if (!r && tune_verbose())
+        std::fprintf(stderr, "libpt autotune %s: INT8 tile %dx%d, K chunk %d B: %.3f ms\n",
+                     key.c_str(), TC_BM, tiles[t].bn, tiles[t].kc, ms);
+      if (!r && (t == 0 || ms < best_ms)) {
+        best = t;
+        best_ms = ms;
+      }
+    }
+    if (r) return r;
+    p->i8tile = tiles[best];
+    for (SpinCase &c : p->cases)
+      if (c.count)
+        if ((r = i8_encode(p, c))) return r;
+    choice.assign(1, best);
+  } else {
+    choice.assign(p->cases.size(), 0);
+    for (size_t ci = 0; ci < p->cases.size() && !r; ++ci) {
+      SpinCase &c = p->cases[ci];
+      if (!c.count) continue;
+      const std::vector<int64_t> ents = probe_of(c);
+      const int start = c.bm;
+      int best = start;
+      float best_ms = 0.f;
+      for (int bm : {start, start == 96 ? 128 : 96}) {
+        if ((r = set_bm(c, bm))) break;
+        float ms = 0.f;
+        if ((r = probe_ms(p, c, ents, &ms))) break;
+        if ((r = probe_ms(p, c, ents, &ms))) break;
+        if (tune_verbose())
+          std::fprintf(stderr, "libpt autotune %s: case %zu, DMMA tile rows %d: %.3f ms\n",
+                       key.c_str(), ci, bm, ms);
+        if (bm == start || ms < best_ms) {
+          best = bm;
+          best_ms = ms;
+        }
+      }
+      if (!r) r = set_bm(c, best);
+      choice[ci] = best;
+    }
+    if (r) return r;
+  }
+  tune_store(key, choice);
+  p->launches = 0;
+  // forget the probe's energies
+  CK(cudaMemsetAsync(p->e_slot, 0, (p->queue.size() + 1) * 8, p->st));
+  CK(cudaStreamSynchronize(p->st));
   return LIBPT_OK;
 }
 
@@ -1109,6 +1261,10 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
   p->dtype = dtype;
   p->precision = precision;
   p->slices = slices;
+  {
+    const I8Tile *t = nullptr;
+    if (i8_tiles(slices, &t) > 0) p->i8tile = t[0];   // widest tile
+  }
   p->st = st;
   p->factor = unr ? 1.0 : 2.0;   // src/pt.c:478, 534, 971, 1049
   p->arena = static_cast<char *>(arena);
@@ -1226,6 +1382,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     p->ws_budget = std::min<size_t>(std::max<size_t>(fr / 2, (size_t)64 << 20),
                                     (size_t)16 << 30);
   } while (0);
+  if (!r) r = autotune(p);
   if (r) {
     plan_destroy(p);
     return r;

@@ -85,7 +85,9 @@ struct SpinCase {
   double flops_per_triple = 0.0;        // reference GEMM flops
   int bm = GEMM_BM;                     // CTA tile rows of this case's GEMMs
   OpDesc opd[MAX_MAPS];                 // operand behind each DMMA map
-  TcMapSet tcmaps;                      // tensor-core views (map 2i, 2i+1)
+  TcMapSet tcmaps;                      // tensor-core views (TF32: map 2i,
+                                        // 2i+1; emulated FP64: map i)
+  signed char *i8pl[MAX_MAPS] = {};     // digit planes behind INT8 map i
 };
 
 }  // namespace ptb
@@ -124,6 +126,7 @@ struct libpt_plan {
   std::vector<std::pair<std::pair<const double *, int>, ptb::Planes>> planes;
   // emulated FP64: digit planes per (source block, role), scale families
   int slices = 6;
+  ptb::I8Tile i8tile{64, 32};           // emulated FP64 tile variant
   std::vector<std::pair<std::pair<const double *, int>, signed char *>> i8planes;
   std::vector<ptb::Family> fams;
   // kernel timing (libpt_plan_timing): events around each launch
@@ -150,11 +153,12 @@ int tc_map_a(CUtensorMap *m, const float *p, int64_t K, int64_t R, int64_t Q,
              int64_t P);
 int tc_map_b(CUtensorMap *m, const float *p, int64_t K, int64_t N, int64_t P);
 // INT8 digit-plane views: A planes [2S][P][Q][R][kpi] as (K, R, Q, P, 2S),
-// B planes [S][P][N][kpi] as (K, N, P, S); kpi = K rounded up to 16.
+// B planes [S][P][N][kpi] as (K, N, P, S); kpi = K rounded up to 16.  Boxes
+// of kc bytes (32 or 64, swizzled to kc) x 128 (A) or bn (B) rows.
 int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
-             int64_t Q, int64_t P, int S);
+             int64_t Q, int64_t P, int S, int kc);
 int i8_map_b(CUtensorMap *m, const signed char *p, int64_t K, int64_t N,
-             int64_t P, int S);
+             int64_t P, int S, int kc, int bn);
 // DMMA views of padded FP64 blocks: A [P][Q][R][pad4(K)], B [P][K][Nld].
 int dmma_map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R,
                int64_t Q, int64_t P, int bm);

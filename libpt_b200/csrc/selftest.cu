@@ -39,16 +39,22 @@ __global__ void fill_kernel(double *x, int64_t rows, int64_t w, int64_t ld,
   }
 }
 
+// C = A (B1 - B2) and its magnitude sum |A| (|B1| + |B2|), the scale that
+// bounds a dot product's rounding error.
 __global__ void ref_kernel(const double *A, const double *B1, const double *B2,
-                           double *C, int m, int n, int k, int64_t lda,
-                           int64_t ldb) {
+                           double *C, double *Cabs, int m, int n, int k,
+                           int64_t lda, int64_t ldb) {
   const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (idx >= (int64_t)m * n) return;
   const int r = (int)(idx / n), c = (int)(idx % n);
-  double s = 0.0;
-  for (int x = 0; x < k; ++x)
-    s += A[r * lda + x] * (B1[x * ldb + c] - B2[x * ldb + c]);
+  double s = 0.0, t = 0.0;
+  for (int x = 0; x < k; ++x) {
+    const double a = A[r * lda + x], b1 = B1[x * ldb + c], b2 = B2[x * ldb + c];
+    s += a * (b1 - b2);
+    t += fabs(a) * (fabs(b1) + fabs(b2));
+  }
   C[r * ldb + c] = s;
+  Cabs[r * ldb + c] = t;
 }
 
 ptb::TcMapSet &tcmaps_scratch() {
@@ -62,12 +68,18 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
                              double *rel_err) {
   using namespace ptb;
   int slices = (precision >> 8) & 0xFF;
+  const int variant = (precision >> 16) & 0xFF;
   precision &= 0xFF;
   if (slices == 0) slices = 6;
+  const I8Tile *tiles = nullptr;
+  const int ntiles = i8_tiles(slices, &tiles);
+  const int nvar = precision == LIBPT_PREC_FP64    ? 2
+                   : precision == LIBPT_PREC_EMU64 ? ntiles
+                                                   : 1;
   if (!rel_err || m < 1 || n < 1 || k < 1 || m > 4096 || n > 4096 ||
       k > 4096 || slices < TC_S_MIN || slices > TC_S_MAX ||
       (precision != LIBPT_PREC_FP64 && precision != LIBPT_PREC_TF32X3 &&
-       precision != LIBPT_PREC_EMU64)) {
+       precision != LIBPT_PREC_EMU64) || variant >= nvar) {
     set_error("libpt_selftest: bad arguments");
     return LIBPT_ERR_ARG;
   }
@@ -88,9 +100,10 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
   double *B2 = (double *)alloc((size_t)k * np * 8);
   double *Cm = (double *)alloc((size_t)m * np * 8);
   double *Cr = (double *)alloc((size_t)m * np * 8);
+  double *Ca = (double *)alloc((size_t)m * np * 8);
   unsigned *err = (unsigned *)alloc(4);
   GemmJob *dj = (GemmJob *)alloc(sizeof(GemmJob));
-  if (!A || !B1 || !B2 || !Cm || !Cr || !err || !dj) {
+  if (!A || !B1 || !B2 || !Cm || !Cr || !Ca || !err || !dj) {
     set_error("libpt_selftest: cudaMalloc failed");
     return done(LIBPT_ERR_NOMEM);
   }
@@ -100,8 +113,8 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
   fill_kernel<<<256, 256>>>(B2, k, n, np, 3, full);
   cudaMemset(Cm, 0, (size_t)m * np * 8);
   cudaMemset(err, 0, 4);
-  ref_kernel<<<(unsigned)(((int64_t)m * n + 255) / 256), 256>>>(A, B1, B2, Cr, m,
-                                                               n, k, kp, np);
+  ref_kernel<<<(unsigned)(((int64_t)m * n + 255) / 256), 256>>>(
+      A, B1, B2, Cr, Ca, m, n, k, kp, np);
   GemmJob job;
   memset(&job, 0, sizeof(job));
   job.out = Cm;
@@ -114,11 +127,12 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
   if (precision == LIBPT_PREC_FP64) {
     MapSet maps;
     memset(&maps, 0, sizeof(maps));
-    if ((r = dmma_map_a(&maps.m[0], A, k, m, 1, 1, 128)) ||
+    const int bm = variant ? 96 : 128;
+    if ((r = dmma_map_a(&maps.m[0], A, k, m, 1, 1, bm)) ||
         (r = dmma_map_b(&maps.m[1], B1, n, np, k, 1)) ||
         (r = dmma_map_b(&maps.m[2], B2, n, np, k, 1)))
       return done(r);
-    job.mtiles = (m + 127) / 128;
+    job.mtiles = (m + bm - 1) / bm;
     job.ntiles_n = (int)((np + GEMM_BN - 1) / GEMM_BN);
     for (int s = 0; s < 2; ++s) {
       job.seg[s].amap = 0;
@@ -127,7 +141,7 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
       job.seg[s].ksteps = (k + GEMM_BK - 1) / GEMM_BK;
     }
     cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
-    ce = gemm_dmma_launch(maps, dj, 1, job.mtiles * job.ntiles_n, 128, err,
+    ce = gemm_dmma_launch(maps, dj, 1, job.mtiles * job.ntiles_n, bm, err,
                           nullptr);
   } else if (precision == LIBPT_PREC_EMU64) {
     // one A family (A itself) and one B family (B1 part 0, B2 part 1)
@@ -161,26 +175,27 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
       set_error(cudaGetErrorString(ce));
       return done(LIBPT_ERR_CUDA);
     }
-    if ((r = i8_map_a(&(tcmaps_scratch().m[0]), pa, k, m, 1, 1, S)) ||
-        (r = i8_map_b(&(tcmaps_scratch().m[1]), pb1, k, np, 1, S)) ||
-        (r = i8_map_b(&(tcmaps_scratch().m[2]), pb2, k, np, 1, S)))
+    const I8Tile tl = tiles[variant];
+    if ((r = i8_map_a(&(tcmaps_scratch().m[0]), pa, k, m, 1, 1, S, tl.kc)) ||
+        (r = i8_map_b(&(tcmaps_scratch().m[1]), pb1, k, np, 1, S, tl.kc,
+                      tl.bn)) ||
+        (r = i8_map_b(&(tcmaps_scratch().m[2]), pb2, k, np, 1, S, tl.kc,
+                      tl.bn)))
       return done(r);
     job.mtiles = (m + TC_BM - 1) / TC_BM;
-    job.ntiles_n = (int)((np + TC_I8_BN - 1) / TC_I8_BN);
+    job.ntiles_n = (int)((np + tl.bn - 1) / tl.bn);
     job.ea = ea;
     job.eb = eb;
-    const int kc = tc_kchunk_elems(TC_INT8);
+    const int kc = tl.kc;
     for (int s2 = 0; s2 < 2; ++s2) {
       job.seg[s2].amap = 0;
       job.seg[s2].bmap = (int16_t)(1 + s2);
       job.seg[s2].neg = (int16_t)s2;
       job.seg[s2].ksteps = (k + kc - 1) / kc;
     }
-    TcProducts pr;
-    memset(&pr, 0, sizeof(pr));
     cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
-    ce = gemm_tc_launch(TC_INT8, tcmaps_scratch(), dj, 1,
-                        job.mtiles * job.ntiles_n, pr, err, nullptr, S);
+    ce = gemm_i8_launch(S, tl, tcmaps_scratch(), dj, 1,
+                        job.mtiles * job.ntiles_n, err, nullptr);
   } else {
     float *pl[6];
     for (int x = 0; x < 6; ++x) {
@@ -233,15 +248,17 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
   }
   unsigned herr = 0;
   cudaMemcpy(&herr, err, 4, cudaMemcpyDeviceToHost);
-  std::vector<double> hm((size_t)m * np), hr((size_t)m * np);
+  std::vector<double> hm((size_t)m * np), hr((size_t)m * np),
+      ha((size_t)m * np);
   cudaMemcpy(hm.data(), Cm, hm.size() * 8, cudaMemcpyDeviceToHost);
   cudaMemcpy(hr.data(), Cr, hr.size() * 8, cudaMemcpyDeviceToHost);
+  cudaMemcpy(ha.data(), Ca, ha.size() * 8, cudaMemcpyDeviceToHost);
   double dmax = 0.0, rmax = 0.0;
   for (int i = 0; i < m; ++i)
     for (int j = 0; j < n; ++j) {
       const size_t x = (size_t)i * np + j;
       dmax = std::max(dmax, std::fabs(hm[x] - hr[x]));
-      rmax = std::max(rmax, std::fabs(hr[x]));
+      rmax = std::max(rmax, ha[x]);
     }
   *rel_err = rmax > 0 ? dmax / rmax : dmax;
   if (herr) {
@@ -249,4 +266,18 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
     return done(LIBPT_ERR_TIMEOUT);
   }
   return done(LIBPT_OK);
+}
+
+LIBPT_API int libpt_selftest_variants(int precision) {
+  int slices = (precision >> 8) & 0xFF;
+  if (slices == 0) slices = 6;
+  switch (precision & 0xFF) {
+    case LIBPT_PREC_FP64: return 2;
+    case LIBPT_PREC_TF32X3: return 1;
+    case LIBPT_PREC_EMU64: {
+      const ptb::I8Tile *t = nullptr;
+      return ptb::i8_tiles(slices, &t);
+    }
+    default: return 0;
+  }
 }

@@ -87,6 +87,8 @@ def lib():
         ctypes.POINTER(ctypes.c_int64)]
     L.libpt_selftest.restype = ctypes.c_int
     L.libpt_selftest.argtypes = [ctypes.c_int] * 4 + [dp]
+    L.libpt_selftest_variants.restype = ctypes.c_int
+    L.libpt_selftest_variants.argtypes = [ctypes.c_int]
     L.libpt_plan_destroy.restype = ctypes.c_int
     L.libpt_plan_destroy.argtypes = [vp]
     _lib = L
@@ -129,12 +131,18 @@ def solve_device(case, tensors, mp=False, stream=None):
     return e.value
 
 
-def selftest(precision, m, n, k):
-    """Relative error of one contraction kernel against an FP64 product
-    (libpt_selftest)."""
+def selftest(precision, m, n, k, variant=0):
+    """Error of one contraction kernel (tile variant `variant`) against an
+    FP64 product, over the dot products' magnitude scale (libpt_selftest)."""
     e = ctypes.c_double(-1.0)
-    check(lib().libpt_selftest(precision, m, n, k, ctypes.byref(e)))
+    check(lib().libpt_selftest(precision | (variant << 16), m, n, k,
+                               ctypes.byref(e)))
     return e.value
+
+
+def selftest_variants(precision):
+    """Number of tile variants of a precision mode (libpt_selftest_variants)."""
+    return lib().libpt_selftest_variants(precision)
 
 
 class Plan:

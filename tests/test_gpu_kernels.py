@@ -11,25 +11,35 @@ SHAPES = [(128, 256, 32), (1, 1, 1), (5, 7, 3), (200, 300, 100),
           (477, 1000, 477), (96, 130, 45), (300, 520, 700)]
 
 
+@pytest.mark.parametrize("variant", [0, 1])       # 128-row, 96-row tiles
 @pytest.mark.parametrize("m,n,k", SHAPES)
-def test_dmma_fp64(m, n, k):
-    assert ffi.selftest(ffi.PREC_FP64, m, n, k) < 1e-13
+def test_dmma_fp64(m, n, k, variant):
+    assert ffi.selftest(ffi.PREC_FP64, m, n, k, variant) < 1e-14
 
 
 @pytest.mark.parametrize("m,n,k", SHAPES)
 def test_tcgen05_tf32x3(m, n, k):
     # 3xTF32 keeps ~21 bits per product and the tensor cores accumulate in
-    # FP32: measured 2e-7 .. 1.1e-5 of max|C| for k <= 700
+    # FP32 (truncating): about 1.6e-8 per accumulation step
     assert ffi.selftest(ffi.PREC_TF32X3, m, n, k) < 5e-5
 
 
-# emulated FP64: each 7-bit digit slice gains a factor 2^7 (measured:
-# S=4 8e-9, S=5 6e-11, S=6 5e-13, S=7 5e-15 of max|C|)
-EMU_BOUND = {4: 2e-8, 5: 2e-10, 6: 2e-12, 7: 2e-14}
+# emulated FP64: each 7-bit digit slice gains a factor 2^7.  The S(S+1)/2
+# kept digit products leave (S+1) 2^(-7S-2) of |a||b| per product and each
+# operand's truncation 2^(-7S-1); with row / column scales up to 4x the
+# values, the error over sum |a||b| stays below 2^(-7S+6)
+EMU_BOUND = {s: 2.0 ** (-7 * s + 6) for s in (4, 5, 6, 7)}
 
 
-@pytest.mark.parametrize("slices", [4, 5, 6, 7])
+# every compiled INT8 tile variant (tile width x K chunk) of each slice count
+I8_VARIANTS = {4: 4, 5: 4, 6: 3, 7: 1}
+
+
+@pytest.mark.parametrize("slices,variant",
+                         [(s, t) for s, n in I8_VARIANTS.items()
+                          for t in range(n)])
 @pytest.mark.parametrize("m,n,k", SHAPES[1:])
-def test_tcgen05_int8_emulated_fp64(slices, m, n, k):
+def test_tcgen05_int8_emulated_fp64(slices, variant, m, n, k):
     prec = ffi.PREC_EMU64 | (slices << 8)
-    assert ffi.selftest(prec, m, n, k) < EMU_BOUND[slices]
+    assert ffi.selftest_variants(prec) == I8_VARIANTS[slices]
+    assert ffi.selftest(prec, m, n, k, variant) < EMU_BOUND[slices]
