@@ -126,6 +126,14 @@ int libpt_selftest(int precision, int m, int n, int k, double *rel_err);
 /* Number of tile variants libpt_selftest accepts for a precision (with its
  * slice count in bits 8-15).  No counterpart in the reference. */
 int libpt_selftest_variants(int precision);
+/* Contraction-kernel microbenchmark: the libpt_selftest job (m x k by
+ * k x n, two segments, operands resident in device memory; n up to 2^20
+ * with n*k <= 2^27 and m*n <= 2^25) checked once, then launched reps times;
+ * writes the mean
+ * device time of one launch (ms) and the check's error (rel_err, may be
+ * NULL).  The job does 4*m*n*k flops.  No counterpart in the reference. */
+int libpt_kernel_bench(int precision, int m, int n, int k, int reps,
+                       double *ms, double *rel_err);
 
 /* ---- device-pointer twins ----------------------------------------------
  * Same arguments as the reference entry points, but every tensor is a

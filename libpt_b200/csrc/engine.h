@@ -90,13 +90,17 @@ cudaError_t gemm_tc_launch(int kind, const TcMapSet &maps,
 //
 // S digit planes per operand, the products with p + q <= S - 1 (0-based)
 // into S INT32 accumulators of bn columns.  The digit planes are a
-// coordinate of one map per operand: A maps [2S][P][Q][R][kpi] hold the
-// digits then their negatives, B maps [S][P][N][kpi]; both viewed with
-// boxes of kc bytes x (128 | bn) rows, swizzled to kc bytes.
+// coordinate of one map per operand: A maps [2S][P][Q][kpi/32][R][32] hold
+// the digits then their negatives, B maps [S][P][kpi/32][N][32]; 32-byte K
+// chunks of 128 (A) or bn (B) rows are contiguous, read as one TMA box each
+// and swizzled to 32 bytes.  An A segment's (Q, P) coordinates are merged
+// into a_q = a_p * Q + a_q.
 struct I8Tile {
   int bn;   // tile columns (multiple of 16, S * bn <= 512)
-  int kc;   // K bytes per pipeline stage (32 or 64)
+  int kc;   // K bytes per pipeline stage (32 or 64: one or two MMA K steps)
 };
+// K padded to whole 32-byte chunks: the row extent of the digit planes.
+inline int64_t i8_kpad(int64_t K) { return (K + 31) & ~int64_t(31); }
 // The tile variants compiled for a slice count (widest first); returns
 // their number (0 for an unsupported count).
 int i8_tiles(int slices, const I8Tile **out);

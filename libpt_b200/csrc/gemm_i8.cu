@@ -10,20 +10,26 @@
 // of BN columns; S * BN <= 512).  Subtracted segments read the negated
 // digit planes (A planes S..2S-1), so all products accumulate with +.
 //
-// Tile variants (BN columns, KC bytes of K per pipeline stage): the B200
-// feeds an M=128 INT8 MMA from shared memory at (128 + BN) * 32 bytes per
+// Tile variants (BN columns, KC = 32 or 64 bytes of K per pipeline stage):
+// an M=128 INT8 MMA reads (128 + BN) * 32 bytes of shared memory per
 // 128 * BN * 32 multiply-adds, so wider tiles relieve shared memory and L2;
-// narrower K chunks allow more stages in flight.  The plan's autotuner
-// times the variants of its slice count and keeps the fastest.
+// one K step per stage allows more stages in flight.  The digit planes are
+// stored in 32-byte K chunks of contiguous rows, so every TMA box (32 bytes
+// x 128 or BN rows) is one contiguous block: L2 serves it in whole lines
+// (row-strided 32-byte boxes cost one L2 tag request per row).  The plan's
+// autotuner times the variants of its slice count and keeps the fastest.
 //
 // Warp roles (persistent CTA, one per SM):
 //   warp 0      TMA producer: the S A planes and S B planes of one K chunk
-//               per stage (swizzled to KC bytes, K-major)
+//               per stage (32-byte boxes swizzled to 32 bytes, K-major)
 //   warp 1      TMEM owner and MMA issuer (one thread): S(S+1)/2 products
 //               per K step; tcgen05.commit frees the stage
-//   warps 2-5   epilogue: tcgen05.ld of the S accumulators, combined exactly
+//   warps 2-9   epilogue: tcgen05.ld of the S accumulators, combined exactly
 //               in 64-bit integers into two partial sums, one FP64 rounding,
-//               an exact power-of-two scale, FP64 store
+//               an exact power-of-two scale, FP64 store.  Two warps per TMEM
+//               lane quarter split the tile's 16-column chunks, so the drain
+//               (during which the single-buffered accumulators hold up the
+//               next tile's MMAs) takes half as long.
 // All mbarrier waits are bounded; on expiry the kernel records the error,
 // stops issuing, still releases TMEM, and returns.
 #include "common.cuh"
@@ -115,9 +121,13 @@ constexpr int pow2_cols(int c) {
 
 template <int S, int BN, int KC>
 struct I8Cfg {
-  static constexpr int A_TILE = BM * KC;                       // per plane
-  static constexpr int B_TILE = (BN * KC + 1023) / 1024 * 1024;
+  static constexpr int KS = KC / 32;                  // MMA K steps per stage
+  static constexpr int A_SUB = BM * 32;               // one 32-byte K step
+  static constexpr int B_SUB = (BN * 32 + 1023) / 1024 * 1024;
+  static constexpr int A_TILE = KS * A_SUB;           // per plane and stage
+  static constexpr int B_TILE = KS * B_SUB;
   static constexpr int STAGE = S * (A_TILE + B_TILE);
+  static constexpr int TX = S * KS * (A_SUB + BN * 32);   // bytes TMA writes
   static constexpr int ST0 = (227 * 1024 - 1024 - 256) / STAGE;
   static constexpr int ST = ST0 > 8 ? 8 : ST0;                 // stages
   static constexpr int TMEM_COLS = pow2_cols(S * BN);
@@ -130,8 +140,11 @@ struct I8Cfg {
   static_assert(A_TILE % 1024 == 0, "plane tiles keep 1 KiB alignment");
 };
 
+constexpr int I8_THREADS = 320;   // producer, MMA issuer, 8 epilogue warps
+constexpr int I8_EPI_THREADS = 256;
+
 template <int S, int BN, int KC>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(I8_THREADS, 1)
     gemm_i8_kernel(const __grid_constant__ TcMapSet maps,
                    const GemmJob *__restrict__ jobs, int njobs,
                    int total_tiles, unsigned *err) {
@@ -153,7 +166,7 @@ __global__ void __launch_bounds__(192, 1)
       mbar_init(&empty[s], 1);
     }
     mbar_init(accfull, 1);
-    mbar_init(accempty, 128);
+    mbar_init(accempty, I8_EPI_THREADS);
     mbar_fence_init();
   }
   if (warp == 1) {
@@ -186,15 +199,20 @@ __global__ void __launch_bounds__(192, 1)
             ok = false;
             break;
           }
-          mbar_arrive_expect_tx(&full[stage], C::STAGE - S * (C::B_TILE - BN * KC));
+          mbar_arrive_expect_tx(&full[stage], C::TX);
           unsigned char *st_base = smem + stage * C::STAGE;
-          const int k0 = ks * KC;
 #pragma unroll
           for (int p = 0; p < S; ++p) {
-            tma_load_5d(st_base + p * C::A_TILE, &maps.m[sg.amap], &full[stage],
-                        k0, m0, sg.a_q, sg.a_p, p + aoff);
-            tma_load_4d(st_base + S * C::A_TILE + p * C::B_TILE,
-                        &maps.m[sg.bmap], &full[stage], k0, n0, sg.b_p, p);
+#pragma unroll
+            for (int kk = 0; kk < C::KS; ++kk) {
+              const int kc = ks * C::KS + kk;    // 32-byte K chunk
+              tma_load_5d(st_base + p * C::A_TILE + kk * C::A_SUB,
+                          &maps.m[sg.amap], &full[stage], 0, m0, kc, sg.a_q,
+                          p + aoff);
+              tma_load_5d(st_base + S * C::A_TILE + p * C::B_TILE +
+                              kk * C::B_SUB,
+                          &maps.m[sg.bmap], &full[stage], 0, n0, kc, sg.b_p, p);
+            }
           }
           if (++stage == ST) {
             stage = 0;
@@ -229,17 +247,17 @@ __global__ void __launch_bounds__(192, 1)
           const uint32_t sa = smem_u32(smem + stage * C::STAGE);
           const uint32_t sb = sa + S * C::A_TILE;
 #pragma unroll
-          for (int pa = 0; pa < S; ++pa) {
-            const uint64_t da = kmajor_desc<KC>(sa + pa * C::A_TILE);
+          for (int kk = 0; kk < C::KS; ++kk) {
 #pragma unroll
-            for (int pb = 0; pb + pa < S; ++pb) {
-              const int w = pa + pb;     // digit weight 2^-7(w+2)
-              const uint64_t db = kmajor_desc<KC>(sb + pb * C::B_TILE);
+            for (int pa = 0; pa < S; ++pa) {
+              const uint64_t da =
+                  kmajor_desc<32>(sa + pa * C::A_TILE + kk * C::A_SUB);
 #pragma unroll
-              for (int kk = 0; kk < KC / 32; ++kk) {
-                // 32-byte K steps through the swizzled row
-                mma_i8(tmem + (uint32_t)(w * BN), da + (uint64_t)(kk * 2),
-                       db + (uint64_t)(kk * 2), i8_idesc<BN>(),
+              for (int pb = 0; pb + pa < S; ++pb) {
+                const int w = pa + pb;     // digit weight 2^-7(w+2)
+                const uint64_t db =
+                    kmajor_desc<32>(sb + pb * C::B_TILE + kk * C::B_SUB);
+                mma_i8(tmem + (uint32_t)(w * BN), da, db, i8_idesc<BN>(),
                        (started >> w) & 1u);
                 started |= 1u << w;
               }
@@ -257,6 +275,7 @@ __global__ void __launch_bounds__(192, 1)
   } else if (warp >= 2) {
     // ---------------- epilogue ----------------
     const int q = warp & 3;            // TMEM lane quarter of this warp
+    const int half = (warp - 2) >> 2;  // which 16-column chunks it takes
     int it = 0;
     constexpr int H = C::H;
     // weights of the two partial sums: hi counts units of acc_{H-1},
@@ -275,7 +294,7 @@ __global__ void __launch_bounds__(192, 1)
       const int erow = rok ? job.ea[row] : 0;
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
-      for (int c0 = 0; c0 < BN; c0 += 16) {
+      for (int c0 = 16 * half; c0 < BN; c0 += 32) {
         // exact: acc_0..acc_{H-1} and acc_H..acc_{S-1} folded by Horner in
         // base 2^7 into 64-bit integers (|sum| < 2^50 for |acc| < 2^28)
         long long hi[16], lo[16];
@@ -305,17 +324,21 @@ __global__ void __launch_bounds__(192, 1)
             lo[x] = l;
           }
         }
-        if (rok) {
+        if (rok && n0 + c0 < job.N) {
+          // the chunk's 16 column exponents in one aligned 16-byte load (the
+          // exponent arrays carry 16 bytes of padding past their N entries)
+          const int4 ebv = *reinterpret_cast<const int4 *>(job.eb + n0 + c0);
+          const signed char *eb16 = reinterpret_cast<const signed char *>(&ebv);
 #pragma unroll
           for (int x = 0; x < 16; x += 2) {
             const int col = n0 + c0 + x;
             if (col < job.N) {
               // one rounding, then exact power-of-two scales
               const double v0 = fma((double)hi[x], w_hi, (double)lo[x] * w_lo) *
-                                pow2i(erow + job.eb[col]);
+                                pow2i(erow + eb16[x]);
               const double v1 =
                   fma((double)hi[x + 1], w_hi, (double)lo[x + 1] * w_lo) *
-                  pow2i(erow + job.eb[col + 1]);
+                  pow2i(erow + eb16[x + 1]);
               *reinterpret_cast<double2 *>(orow + col) = make_double2(v0, v1);
             }
           }
@@ -349,7 +372,8 @@ cudaError_t launch(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
     configured = true;
   }
   int grid = total_tiles < 148 ? total_tiles : 148;
-  kern<<<grid, 192, C::SMEM, st>>>(maps, d_jobs, njobs, total_tiles, d_err);
+  kern<<<grid, I8_THREADS, C::SMEM, st>>>(maps, d_jobs, njobs, total_tiles,
+                                          d_err);
   return cudaGetLastError();
 }
 

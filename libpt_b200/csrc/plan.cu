@@ -145,24 +145,26 @@ int dalloc(libpt_plan *p, void **ptr, size_t bytes);
 
 }  // namespace
 
+// Digit-plane views (see slice_a / slice_b): 32-byte K chunks of rows
+// stored contiguously, boxes of 32 bytes x 128 (A) or bn (B) rows swizzled
+// to 32 bytes.  A: (32, R, nK, Q*P, 2S); B: (32, N, nK, P, S).
 int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
-             int64_t Q, int64_t P, int S, int kc) {
+             int64_t Q, int64_t P, int S) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
     return LIBPT_ERR_CUDA;
   }
-  const int64_t kpi = (K + 15) & ~int64_t(15);
-  cuuint64_t dims[5] = {(cuuint64_t)K, (cuuint64_t)R, (cuuint64_t)Q,
-                        (cuuint64_t)P, (cuuint64_t)(2 * S)};
-  cuuint64_t str[4] = {(cuuint64_t)kpi, (cuuint64_t)(R * kpi),
-                       (cuuint64_t)(Q * R * kpi), (cuuint64_t)(P * Q * R * kpi)};
-  cuuint32_t box[5] = {(cuuint32_t)kc, (cuuint32_t)TC_BM, 1, 1, 1};
+  const int64_t kpi = i8_kpad(K), nk = kpi / 32, npq = Q * P;
+  cuuint64_t dims[5] = {32, (cuuint64_t)R, (cuuint64_t)nk, (cuuint64_t)npq,
+                        (cuuint64_t)(2 * S)};
+  cuuint64_t str[4] = {32, (cuuint64_t)(R * 32), (cuuint64_t)(R * kpi),
+                       (cuuint64_t)(npq * R * kpi)};
+  cuuint32_t box[5] = {32, (cuuint32_t)TC_BM, 1, 1, 1};
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, (void *)p, dims, str,
                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   kc == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled (INT8 A view) failed: " +
@@ -173,23 +175,22 @@ int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
 }
 
 int i8_map_b(CUtensorMap *m, const signed char *p, int64_t K, int64_t N,
-             int64_t P, int S, int kc, int bn) {
+             int64_t P, int S, int bn) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
     return LIBPT_ERR_CUDA;
   }
-  const int64_t kpi = (K + 15) & ~int64_t(15);
-  cuuint64_t dims[4] = {(cuuint64_t)K, (cuuint64_t)N, (cuuint64_t)P,
+  const int64_t kpi = i8_kpad(K), nk = kpi / 32;
+  cuuint64_t dims[5] = {32, (cuuint64_t)N, (cuuint64_t)nk, (cuuint64_t)P,
                         (cuuint64_t)S};
-  cuuint64_t str[3] = {(cuuint64_t)kpi, (cuuint64_t)(N * kpi),
+  cuuint64_t str[4] = {32, (cuuint64_t)(N * 32), (cuuint64_t)(N * kpi),
                        (cuuint64_t)(P * N * kpi)};
-  cuuint32_t box[4] = {(cuuint32_t)kc, (cuuint32_t)bn, 1, 1};
-  cuuint32_t es[4] = {1, 1, 1, 1};
-  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, (void *)p, dims, str,
+  cuuint32_t box[5] = {32, (cuuint32_t)bn, 1, 1, 1};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, (void *)p, dims, str,
                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   kc == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled (INT8 B view) failed: " +
@@ -819,9 +820,9 @@ int i8_encode(libpt_plan *p, SpinCase &c) {
     const int r =
         d.role == 0
             ? i8_map_a(&c.tcmaps.m[i], c.i8pl[i], d.K, d.R, d.Q, d.P,
-                       p->slices, p->i8tile.kc)
+                       p->slices)
             : i8_map_b(&c.tcmaps.m[i], c.i8pl[i], d.K, d.N, d.P, p->slices,
-                       p->i8tile.kc, p->i8tile.bn);
+                       p->i8tile.bn);
     if (r) return r;
   }
   return LIBPT_OK;
@@ -836,7 +837,7 @@ int i8_planes(libpt_plan *p, SpinCase &c) {
     if (!f) return LIBPT_ERR_NOMEM;
     const int set = (d.fam % 100) / 8;
     const int k = (set ? p->R : p->L).balance;
-    const int64_t kpi = (d.K + 15) & ~int64_t(15);
+    const int64_t kpi = i8_kpad(d.K);
     const std::pair<const double *, int> key(d.src, d.role);
     signed char *pl = nullptr;
     for (auto &e : p->i8planes)
@@ -998,6 +999,10 @@ int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
           gs.neg = st.neg;
           gs.a_q = ijk[st.aq];
           gs.a_p = ijk[st.ap];
+          if (i8) {   // INT8 A views merge (Q, P) into one coordinate
+            gs.a_q = gs.a_p * (int32_t)c.opd[st.amap].Q + gs.a_q;
+            gs.a_p = 0;
+          }
           gs.b_p = ijk[st.bp];
           gs.ksteps = tc ? (st.k + tc_kchunk_elems(TC_TF32) - 1) /
                                tc_kchunk_elems(TC_TF32)

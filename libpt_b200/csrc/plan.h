@@ -152,13 +152,14 @@ size_t rpt_arena_bytes(int64_t o, int64_t v, int64_t nb);
 int tc_map_a(CUtensorMap *m, const float *p, int64_t K, int64_t R, int64_t Q,
              int64_t P);
 int tc_map_b(CUtensorMap *m, const float *p, int64_t K, int64_t N, int64_t P);
-// INT8 digit-plane views: A planes [2S][P][Q][R][kpi] as (K, R, Q, P, 2S),
-// B planes [S][P][N][kpi] as (K, N, P, S); kpi = K rounded up to 16.  Boxes
-// of kc bytes (32 or 64, swizzled to kc) x 128 (A) or bn (B) rows.
+// INT8 digit-plane views: A planes [2S][P][Q][kpi/32][R][32] as
+// (32, R, kpi/32, Q*P, 2S), B planes [S][P][kpi/32][N][32] as
+// (32, N, kpi/32, P, S); kpi = i8_kpad(K).  Boxes of 32 bytes x 128 (A) or
+// bn (B) rows, swizzled to 32 bytes.
 int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
-             int64_t Q, int64_t P, int S, int kc);
+             int64_t Q, int64_t P, int S);
 int i8_map_b(CUtensorMap *m, const signed char *p, int64_t K, int64_t N,
-             int64_t P, int S, int kc, int bn);
+             int64_t P, int S, int bn);
 // DMMA views of padded FP64 blocks: A [P][Q][R][pad4(K)], B [P][K][Nld].
 int dmma_map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R,
                int64_t Q, int64_t P, int bm);

@@ -240,8 +240,10 @@ __device__ __forceinline__ void digits(double s, int S, signed char *d) {
   }
 }
 
-// A side: src[npq][R][kp] (FP64) -> out[2S][npq][R][kpi] int8: digit planes
-// of a * scale * 2^-ea[x], then their negatives.
+// A side: src[npq][R][kp] (FP64) -> out[2S][npq][kpi/32][R][32] int8: digit
+// planes of a * scale * 2^-ea[x], then their negatives.  Each 32-byte K
+// chunk of R rows is contiguous, so a tensor-core tile's TMA box is one
+// contiguous block of memory.
 __global__ void slice_a_kernel(const double *__restrict__ src, int64_t npq,
                                int64_t R, int64_t K, int64_t kp, int64_t kpi,
                                double scale, const signed char *ea, int S,
@@ -249,19 +251,22 @@ __global__ void slice_a_kernel(const double *__restrict__ src, int64_t npq,
   const int64_t n = npq * R * kpi, plane = n;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = i / kpi, k = i - r * kpi;
-    const double a = k < K ? src[r * kp + k] : 0.0;
+    const int64_t rr = i / kpi, k = i - rr * kpi;
+    const int64_t pq = rr / R, r = rr - pq * R;
+    const double a = k < K ? src[rr * kp + k] : 0.0;
     signed char d[8];
-    digits(ldexp(a * scale, -ea[r % R]), S, d);
+    digits(ldexp(a * scale, -ea[r]), S, d);
+    const int64_t o = pq * R * kpi + ((k >> 5) * R + r) * 32 + (k & 31);
     for (int q = 0; q < S; ++q) {
-      out[q * plane + i] = d[q];
-      out[(S + q) * plane + i] = (signed char)(-d[q]);
+      out[q * plane + o] = d[q];
+      out[(S + q) * plane + o] = (signed char)(-d[q]);
     }
   }
 }
 
 // B side, transposed: B[P][K][N] (row-padded N, see bsrc_col) ->
-// out[S][P][N][kpi] int8 digit planes of b * scale * 2^-eb[n].
+// out[S][P][kpi/32][N][32] int8 digit planes of b * scale * 2^-eb[n]
+// (32-byte K chunks of N columns contiguous).
 __global__ void slice_b_kernel(const double *__restrict__ src, int K,
                                int64_t N, int64_t w, int64_t wsrc,
                                int64_t ldsrc, int64_t kpi, double scale,
@@ -286,7 +291,7 @@ __global__ void slice_b_kernel(const double *__restrict__ src, int K,
     if (n < N && k < kpi) {
       signed char d[8];
       digits(ldexp(t[threadIdx.x][rr] * scale, -eb[n]), S, d);
-      const int64_t o = (p * N + n) * kpi + k;
+      const int64_t o = p * N * kpi + ((int64_t)(k >> 5) * N + n) * 32 + (k & 31);
       for (int q = 0; q < S; ++q) out[q * plane + o] = d[q];
     }
   }

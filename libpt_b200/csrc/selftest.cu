@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -64,8 +65,13 @@ ptb::TcMapSet &tcmaps_scratch() {
 
 }  // namespace
 
-LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
-                             double *rel_err) {
+namespace {
+
+// One contraction job on random operands: checked against the FP64
+// reference (rel_err), then, when reps > 0, launched reps more times and
+// timed with CUDA events (ms: mean device time of one launch).
+int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
+                double *ms) {
   using namespace ptb;
   int slices = (precision >> 8) & 0xFF;
   const int variant = (precision >> 16) & 0xFF;
@@ -76,8 +82,10 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
   const int nvar = precision == LIBPT_PREC_FP64    ? 2
                    : precision == LIBPT_PREC_EMU64 ? ntiles
                                                    : 1;
-  if (!rel_err || m < 1 || n < 1 || k < 1 || m > 4096 || n > 4096 ||
-      k > 4096 || slices < TC_S_MIN || slices > TC_S_MAX ||
+  if (!rel_err || m < 1 || n < 1 || k < 1 || m > 4096 || n > (1 << 20) ||
+      k > 4096 || (int64_t)n * k > ((int64_t)1 << 27) ||
+      (int64_t)m * n > ((int64_t)1 << 25) || reps < 0 ||
+      slices < TC_S_MIN || slices > TC_S_MAX ||
       (precision != LIBPT_PREC_FP64 && precision != LIBPT_PREC_TF32X3 &&
        precision != LIBPT_PREC_EMU64) || variant >= nvar) {
     set_error("libpt_selftest: bad arguments");
@@ -124,6 +132,7 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
   job.nseg = 2;
   int r = LIBPT_OK;
   cudaError_t ce = cudaSuccess;
+  std::function<cudaError_t()> launch;
   if (precision == LIBPT_PREC_FP64) {
     MapSet maps;
     memset(&maps, 0, sizeof(maps));
@@ -141,12 +150,14 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
       job.seg[s].ksteps = (k + GEMM_BK - 1) / GEMM_BK;
     }
     cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
-    ce = gemm_dmma_launch(maps, dj, 1, job.mtiles * job.ntiles_n, bm, err,
-                          nullptr);
+    launch = [=]() {
+      return gemm_dmma_launch(maps, dj, 1, job.mtiles * job.ntiles_n, bm, err,
+                              nullptr);
+    };
   } else if (precision == LIBPT_PREC_EMU64) {
     // one A family (A itself) and one B family (B1 part 0, B2 part 1)
     const int S = slices;
-    const int64_t kpi = (k + 15) & ~int64_t(15);
+    const int64_t kpi = i8_kpad(k);
     unsigned long long *ma = (unsigned long long *)alloc((size_t)m * 8 + 8);
     unsigned long long *mb0 = (unsigned long long *)alloc((size_t)np * 8 + 8);
     unsigned long long *mb1 = (unsigned long long *)alloc((size_t)np * 8 + 8);
@@ -176,11 +187,9 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
       return done(LIBPT_ERR_CUDA);
     }
     const I8Tile tl = tiles[variant];
-    if ((r = i8_map_a(&(tcmaps_scratch().m[0]), pa, k, m, 1, 1, S, tl.kc)) ||
-        (r = i8_map_b(&(tcmaps_scratch().m[1]), pb1, k, np, 1, S, tl.kc,
-                      tl.bn)) ||
-        (r = i8_map_b(&(tcmaps_scratch().m[2]), pb2, k, np, 1, S, tl.kc,
-                      tl.bn)))
+    if ((r = i8_map_a(&(tcmaps_scratch().m[0]), pa, k, m, 1, 1, S)) ||
+        (r = i8_map_b(&(tcmaps_scratch().m[1]), pb1, k, np, 1, S, tl.bn)) ||
+        (r = i8_map_b(&(tcmaps_scratch().m[2]), pb2, k, np, 1, S, tl.bn)))
       return done(r);
     job.mtiles = (m + TC_BM - 1) / TC_BM;
     job.ntiles_n = (int)((np + tl.bn - 1) / tl.bn);
@@ -194,8 +203,10 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
       job.seg[s2].ksteps = (k + kc - 1) / kc;
     }
     cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
-    ce = gemm_i8_launch(S, tl, tcmaps_scratch(), dj, 1,
-                        job.mtiles * job.ntiles_n, err, nullptr);
+    launch = [=]() {
+      return gemm_i8_launch(S, tl, tcmaps_scratch(), dj, 1,
+                            job.mtiles * job.ntiles_n, err, nullptr);
+    };
   } else {
     float *pl[6];
     for (int x = 0; x < 6; ++x) {
@@ -238,9 +249,12 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
     }
     pr.n = 3;
     cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
-    ce = gemm_tc_launch(TC_TF32, maps, dj, 1, job.mtiles * job.ntiles_n, pr,
-                        err, nullptr);
+    launch = [=]() {
+      return gemm_tc_launch(TC_TF32, maps, dj, 1, job.mtiles * job.ntiles_n,
+                            pr, err, nullptr);
+    };
   }
+  if (ce == cudaSuccess) ce = launch();
   if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
   if (ce != cudaSuccess) {
     set_error(std::string("libpt_selftest: ") + cudaGetErrorString(ce));
@@ -265,7 +279,53 @@ LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
     set_error("libpt_selftest: a device-side wait exceeded its time limit");
     return done(LIBPT_ERR_TIMEOUT);
   }
+  if (reps > 0 && ms) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, nullptr);
+    for (int x = 0; x < reps && ce == cudaSuccess; ++x) ce = launch();
+    cudaEventRecord(e1, nullptr);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+    float t = 0.f;
+    if (ce == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ce != cudaSuccess) {
+      set_error(std::string("libpt_kernel_bench: ") + cudaGetErrorString(ce));
+      return done(LIBPT_ERR_CUDA);
+    }
+    *ms = t / reps;
+    cudaMemcpy(&herr, err, 4, cudaMemcpyDeviceToHost);
+    if (herr) {
+      set_error("libpt_kernel_bench: a device-side wait exceeded its limit");
+      return done(LIBPT_ERR_TIMEOUT);
+    }
+  }
   return done(LIBPT_OK);
+}
+
+}  // namespace
+
+LIBPT_API int libpt_selftest(int precision, int m, int n, int k,
+                             double *rel_err) {
+  if (n > 4096) {
+    ptb::set_error("libpt_selftest: n > 4096");
+    return LIBPT_ERR_ARG;
+  }
+  return kernel_case(precision, m, n, k, 0, rel_err, nullptr);
+}
+
+LIBPT_API int libpt_kernel_bench(int precision, int m, int n, int k, int reps,
+                                 double *ms, double *rel_err) {
+  if (!ms || reps < 1) {
+    ptb::set_error("libpt_kernel_bench: bad arguments");
+    return LIBPT_ERR_ARG;
+  }
+  double e = 0.0;
+  const int r = kernel_case(precision, m, n, k, reps, &e, ms);
+  if (rel_err) *rel_err = e;
+  return r;
 }
 
 LIBPT_API int libpt_selftest_variants(int precision) {

@@ -89,6 +89,8 @@ def lib():
     L.libpt_selftest.argtypes = [ctypes.c_int] * 4 + [dp]
     L.libpt_selftest_variants.restype = ctypes.c_int
     L.libpt_selftest_variants.argtypes = [ctypes.c_int]
+    L.libpt_kernel_bench.restype = ctypes.c_int
+    L.libpt_kernel_bench.argtypes = [ctypes.c_int] * 5 + [dp, dp]
     L.libpt_plan_destroy.restype = ctypes.c_int
     L.libpt_plan_destroy.argtypes = [vp]
     _lib = L
@@ -138,6 +140,15 @@ def selftest(precision, m, n, k, variant=0):
     check(lib().libpt_selftest(precision | (variant << 16), m, n, k,
                                ctypes.byref(e)))
     return e.value
+
+
+def kernel_bench(precision, m, n, k, reps=10, variant=0):
+    """(mean ms per launch, check error) of one resident contraction job of
+    4 m n k flops (libpt_kernel_bench)."""
+    ms, e = ctypes.c_double(0.0), ctypes.c_double(-1.0)
+    check(lib().libpt_kernel_bench(precision | (variant << 16), m, n, k, reps,
+                                   ctypes.byref(ms), ctypes.byref(e)))
+    return ms.value, e.value
 
 
 def selftest_variants(precision):
