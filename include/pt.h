@@ -121,6 +121,8 @@ const char *libpt_last_error(void);
  * LIBPT_PREC_EMU64) and bits 16-23 a tile variant: FP64 0 = 128-row,
  * 1 = 96-row tiles; emulated FP64 the index of one of the slice count's
  * INT8 tile shapes (0 = widest); libpt_selftest_variants() counts them.
+ * Bits 24-31 nonzero: the kernel reads its tensor maps from device memory
+ * (the form batched multi-solve launches use) instead of kernel parameters.
  * No counterpart in the reference. */
 int libpt_selftest(int precision, int m, int n, int k, double *rel_err);
 /* Number of tile variants libpt_selftest accepts for a precision (with its

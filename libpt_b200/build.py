@@ -25,8 +25,9 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
 HOST_CXX = "/usr/bin/g++"   # the image's $CXX wrapper lacks some runtime specs
 
 SOURCES = ["gemm_dmma.cu", "gemm_tc.cu", "gemm_i8.cu", "epilogue.cu", "prep.cu",
-           "plan.cu", "tune.cpp", "api.cpp", "noalloc.cu", "selftest.cu"]
-HEADERS = ["common.cuh", "engine.h", "plan.h", "tune.h"]
+           "exec.cu", "plan.cu", "tune.cpp", "api.cpp", "noalloc.cu",
+           "selftest.cu"]
+HEADERS = ["common.cuh", "engine.h", "exec.h", "plan.h", "tune.h"]
 
 
 def _newer(target, deps):

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "engine.h"
+
 namespace ptb {
 
 // Device-side error word (one per launch, in global memory): bit 0 = a
@@ -112,6 +114,50 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map,
       : "memory");
 }
 
+// Makes a tensor map that generic-proxy writes (a host copy, or a previous
+// plan's maps at the same address) put in device memory visible to the TMA
+// unit's tensor-map proxy; issued once per map before this CTA's first TMA
+// through it.
+__device__ __forceinline__ void tmap_acquire(const CUtensorMap *map) {
+  asm volatile(
+      "fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(
+          reinterpret_cast<uint64_t>(map))
+      : "memory");
+}
+
+// Remembers which maps of a job's map array this thread has fenced, so each
+// map is acquired once per CTA (and again only when the array changes).
+struct MapFence {
+  const CUtensorMap *base = nullptr;
+  unsigned long long mask = 0;
+  __device__ __forceinline__ const CUtensorMap *get(const CUtensorMap *b,
+                                                    int idx) {
+    if (b != base) {
+      base = b;
+      mask = 0;
+    }
+    if (!((mask >> idx) & 1ull)) {
+      tmap_acquire(b + idx);
+      mask |= 1ull << idx;
+    }
+    return b + idx;
+  }
+};
+
+// A job's tensor map idx: from the launch's parameter table (PM) or from
+// the job's device-memory maps (fenced once per CTA).
+template <bool PM>
+struct MapSource {
+  const LaunchMaps *pm;
+  MapFence mf;
+  __device__ __forceinline__ explicit MapSource(const LaunchMaps *p) : pm(p) {}
+  __device__ __forceinline__ const CUtensorMap *get(const GemmJob &job,
+                                                    int idx) {
+    if (PM) return &pm->m[job.map0 + idx];
+    return mf.get(job.maps, idx);
+  }
+};
+
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map))
                : "memory");
@@ -131,6 +177,21 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0,
 
 __device__ __forceinline__ double flip_sign(double x, unsigned long long mask) {
   return __longlong_as_double(__double_as_longlong(x) ^ mask);
+}
+
+// Index of the last of `n` entries (sorted by `begin`) whose begin <= x.
+template <typename T>
+__device__ __forceinline__ int find_entry(const T *v, int n, int x,
+                                          int32_t T::*begin) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (v[mid].*begin <= x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
 }
 
 }  // namespace ptb

@@ -36,24 +36,54 @@ struct GemmJob {
   double *out;          // C, row-major with leading dimension ldc
   int64_t ldc;
   int32_t M, N;         // N <= ldc, N % 4 == 0
-  int32_t ntiles_n;     // ceil(N / GEMM_BN)
+  int32_t ntiles_n;     // ceil(N / tile columns)
   int32_t tile_begin;   // first flat tile index of this job in the launch
   int32_t nseg;
   int32_t mtiles;       // ceil(M / BM); tiles are numbered M-tile fastest
   GemmSeg seg[MAX_SEG];
   // emulated FP64: power-of-two exponents of the output rows / columns
   const signed char *ea, *eb;
+  // The tensor maps (TMA views) the segments' amap / bmap index, in one of
+  // two places, chosen per launch: a kernel-parameter table (LaunchMaps,
+  // this job's views from entry map0 on; fastest descriptor access), or
+  // 64-byte aligned CUtensorMaps in device memory at `maps` (any number of
+  // plans per launch, fixed kernel parameters for graph replay; kernels
+  // fence each such map before first use).
+  const CUtensorMap *maps;
+  int32_t map0, pad_;
 };
 
-struct MapSet {
-  CUtensorMap m[MAX_MAPS];
+// Kernel-parameter table of the tensor maps of one launch (12 KiB of
+// parameters: CUDA 12.1+ kernels take up to 32 KiB).
+constexpr int LAUNCH_MAPS = 96;
+struct LaunchMaps {
+  CUtensorMap m[LAUNCH_MAPS];
 };
+
+// Work list of one GEMM launch, read by the kernel from device memory so a
+// launch's parameters (and a captured CUDA graph) stay fixed while the list
+// changes.  Jobs are sorted by tile_begin; ntiles = total tiles.  Kernels
+// also take the jobs array itself as a (restrict) parameter, equal to
+// list->jobs, so the compiler may keep job fields across their stores.
+struct GemmList {
+  const GemmJob *jobs;
+  int32_t njobs, ntiles;
+};
+
+// Persistent grid of the GEMM kernels (one CTA per SM).
+constexpr int GEMM_GRID = 148;
 
 size_t gemm_smem_bytes(int bm);
-// bm: CTA tile rows, 96 or 128 (the A views' box height must match).
-cudaError_t gemm_dmma_launch(const MapSet &maps, const GemmJob *d_jobs,
-                             int njobs, int total_tiles, int bm,
-                             unsigned *d_err, cudaStream_t st);
+// bm: CTA tile rows, 96 or 128 (the A views' box height must match).  The
+// kernels run `grid` persistent CTAs over the list's tiles.  Two forms:
+//   pm != null: the launch's tensor maps and the job / tile counts (njobs,
+//               ntiles) as kernel parameters (direct launches);
+//   pm == null: maps in device memory (GemmJob::maps) and the counts read
+//               from d_list (fixed parameters: CUDA graph replay).
+cudaError_t gemm_dmma_launch(const GemmJob *d_jobs, const GemmList *d_list,
+                             int njobs, int ntiles, const LaunchMaps *pm,
+                             int bm, int grid, unsigned *d_err,
+                             cudaStream_t st);
 
 // ---- tensor-core (tcgen05) GEMM --------------------------------------------
 //
@@ -70,6 +100,10 @@ constexpr int TC_INT8 = 1;
 constexpr int TC_S_MIN = 4, TC_S_MAX = 7;
 constexpr int TC_MAX_MAPS = 48;
 
+struct MapSet {
+  CUtensorMap m[MAX_MAPS];
+};
+
 struct TcMapSet {
   CUtensorMap m[TC_MAX_MAPS];
 };
@@ -81,10 +115,10 @@ struct TcProducts {           // acc[c] += A_plane[pa] * B_plane[pb]^T
 
 int tc_kchunk_elems(int kind);   // K elements per pipeline stage (TF32)
 // 3xTF32: planes {hi, lo} in separate maps (2i, 2i+1), products from prods.
-cudaError_t gemm_tc_launch(int kind, const TcMapSet &maps,
-                           const GemmJob *d_jobs, int njobs, int total_tiles,
-                           const TcProducts &prods, unsigned *d_err,
-                           cudaStream_t st, int slices = 0);
+cudaError_t gemm_tc_launch(const GemmJob *d_jobs, const GemmList *d_list,
+                           int njobs, int ntiles, const LaunchMaps *pm,
+                           int grid, const TcProducts &prods, unsigned *d_err,
+                           cudaStream_t st);
 
 // ---- emulated FP64 (tcgen05 kind::i8, gemm_i8.cu) ---------------------------
 //
@@ -104,9 +138,10 @@ inline int64_t i8_kpad(int64_t K) { return (K + 31) & ~int64_t(31); }
 // The tile variants compiled for a slice count (widest first); returns
 // their number (0 for an unsupported count).
 int i8_tiles(int slices, const I8Tile **out);
-cudaError_t gemm_i8_launch(int slices, I8Tile tile, const TcMapSet &maps,
-                           const GemmJob *d_jobs, int njobs, int total_tiles,
-                           unsigned *d_err, cudaStream_t st);
+cudaError_t gemm_i8_launch(int slices, I8Tile tile, const GemmJob *d_jobs,
+                           const GemmList *d_list, int njobs, int ntiles,
+                           const LaunchMaps *pm, int grid, unsigned *d_err,
+                           cudaStream_t st);
 
 // ---- energy epilogues ------------------------------------------------------
 
@@ -114,15 +149,12 @@ constexpr int EPI_A = 8, EPI_B = 8, EPI_C = 32;   // tile extents a x b x c
 constexpr int EPI_THREADS = 256;
 constexpr int EPI_CS = EPI_C + 2;                 // smem row stride (banks)
 
-// Arguments shared by the same-spin (aaa) and mixed-spin (aab) epilogues.
+// Fixed arguments of one spin case's epilogue (device memory, per plan).
 struct EpiArgs {
-  const double *ws;       // triple t's arrays start at ws + t * ws_stride
-  int64_t ws_stride;
   int64_t offL[3];        // array offsets of the (first) amplitude W / L
   int64_t offR[3];        // offsets of R for (fT); offR[0] < 0 for (T)
   int64_t ld[3];          // leading dims: aaa {ldT}; aab {ldU1, ldU2, ldP}
   int64_t rowU1, rowU2;   // aab: padded inner extents of U1 (vb) and U2 (va)
-  const int *trip;        // i, j, k per triple of the batch
   int oa, va, ob, vb;
   const double *d_a, *d_b;                  // denominators [o][v]
   const double *ov1_a, *ov1_b;              // t1 / l1
@@ -131,20 +163,50 @@ struct EpiArgs {
   const double *ov2_a, *ov2_b;              // f_ov / f2_ov
   const double *g2_ab, *g2_aa;              // t2 / l2 blocks
   int64_t g2_ld_ab, g2_ld_aa;
-  double *partials;       // [ntrip][ntiles]
-  int ntiles;
+  int ntiles;             // CTA tiles of one triple
   const int4 *tiles;      // aaa: (a0, b0, c0); aab: (a0, b0, 0) block pairs
   int ctiles;             // aab: number of c blocks
 };
 
+// One triple of an epilogue launch.
+struct EpiItem {
+  const EpiArgs *args;    // its spin case's arguments
+  const double *ws;       // its contraction outputs
+  double *partials;       // its per-tile partial energies [args->ntiles]
+  int32_t i, j, k;
+  int32_t block_begin;    // first flat CTA tile of this item in the launch
+  int32_t nblk;           // its CTA tiles (args->ntiles)
+  int32_t pad_;
+};
+
+struct EpiList {          // items sorted by block_begin
+  const EpiItem *items;
+  int32_t nitems, nblocks;
+};
+
+// One triple's fixed-order reduction: *dst = sum of partials[0..n).
+struct RedItem {
+  const double *partials;
+  double *dst;
+  int32_t n, pad_;
+};
+
+struct RedList {
+  const RedItem *items;
+  int32_t nitems, pad_;
+};
+
 size_t epi_smem_bytes(bool aab, bool ft);
-cudaError_t epi_aaa_launch(const EpiArgs &a, bool ft, int ntrip,
-                           cudaStream_t st);
-cudaError_t epi_aab_launch(const EpiArgs &a, bool ft, int ntrip,
-                           cudaStream_t st);
-// e_slot[slot[t]] = fixed-order sum of partials[t][0..ntiles).
-cudaError_t reduce_partials_launch(const double *partials, int ntiles,
-                                   int ntrip, const int *slot, double *e_slot,
+// persistent: `grid` CTAs stride over list->nblocks tiles (a fixed grid,
+// for graph replay); otherwise a (max tiles of an item) x (items) grid, one
+// CTA per tile, grid = max tiles and nitems the item count.
+cudaError_t epi_aaa_launch(const EpiList *d_list, bool ft, int grid,
+                           int nitems, bool persistent, cudaStream_t st);
+cudaError_t epi_aab_launch(const EpiList *d_list, bool ft, int grid,
+                           int nitems, bool persistent, cudaStream_t st);
+// CTAs the epilogue keeps resident per SM (for persistent grids).
+int epi_blocks_per_sm(bool aab, bool ft);
+cudaError_t reduce_partials_launch(const RedList *d_list, int grid,
                                    cudaStream_t st);
 
 // ---- operand preparation ---------------------------------------------------

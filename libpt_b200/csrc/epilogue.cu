@@ -16,7 +16,11 @@
 // contiguous in a or b (T[c][ab], U2, P) are staged through shared memory
 // as [x][y][c] rows of EPI_CS = 34 doubles: the fill (8 consecutive y per
 // 8 lanes) and the reads (32 consecutive c) are both free of bank conflicts.
-// Each CTA writes one partial sum; reduce_partials adds them in a fixed order.
+// Each CTA tile writes one partial sum; reduce_partials adds them in a fixed
+// order.  Launches are persistent: a fixed grid strides over the flat tiles
+// of a device-memory item list (EpiList), whose items (triples) may belong
+// to different plans; each item points at its spin case's fixed arguments,
+// which a CTA copies to shared memory.
 #include "common.cuh"
 #include "engine.h"
 
@@ -49,21 +53,42 @@ __device__ double block_sum(double x) {
 // thread needs are issued before they are used (unrolled, branch-free with
 // clamped indices and a validity mask), so many requests are in flight.
 
-template <bool FT>
+// Copies an item's case arguments into shared memory (all threads).
+__device__ __forceinline__ void load_args(EpiArgs &dst, const EpiArgs *src) {
+  static_assert(sizeof(EpiArgs) % 8 == 0, "8-byte words");
+  constexpr int W = (int)(sizeof(EpiArgs) / 8);
+  for (int x = threadIdx.x; x < W; x += blockDim.x)
+    reinterpret_cast<long long *>(&dst)[x] =
+        reinterpret_cast<const long long *>(src)[x];
+  __syncthreads();
+}
+
+template <bool FT, bool LOOP>
 __global__ void __launch_bounds__(EPI_THREADS, 2)
-    epi_aaa_kernel(const EpiArgs p) {
+    epi_aaa_kernel(const EpiList *__restrict__ list) {
   extern __shared__ double sm[];
+  __shared__ EpiArgs p;
   constexpr int S = EPI_A * EPI_B * EPI_CS;
   constexpr int NIT = EPI_A * EPI_C * EPI_B / EPI_THREADS;
   // s3[a_][b_][c_] = T[c][pair(a,b)]  (the R copy follows for (fT))
   double *s3 = sm;
-
-  const int4 tl = p.tiles[blockIdx.x];
+  // LOOP: a fixed grid striding over the flat tiles of all items; else one
+  // CTA per (tile, item) of a 2-D grid
+  int blk = blockIdx.x;
+  if (LOOP && blk >= list->nblocks) return;
+  do {
+  const EpiItem &item =
+      LOOP ? list->items[find_entry(list->items, list->nitems, blk,
+                                    &EpiItem::block_begin)]
+           : list->items[blockIdx.y];
+  const int local = LOOP ? blk - item.block_begin : blk;
+  if (!LOOP && local >= item.nblk) return;
+  load_args(p, item.args);
+  const int4 tl = p.tiles[local];
   const int a0 = tl.x, b0 = tl.y, c0 = tl.z;
-  const int t = blockIdx.y;
-  const int i = p.trip[3 * t], j = p.trip[3 * t + 1], k = p.trip[3 * t + 2];
+  const int i = item.i, j = item.j, k = item.k;
   const int v = p.va, o = p.oa;
-  const double *base = p.ws + (int64_t)t * p.ws_stride;
+  const double *base = item.ws;
   const double *T = base + p.offL[0];
   const double *R = FT ? base + p.offR[0] : nullptr;
   const int64_t ld = p.ld[0];
@@ -154,27 +179,43 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
     if (ok_[b_]) e += (w_[b_] - x_[b_]) * r / d_[b_];
   }
   const double s = block_sum(e);
-  if (threadIdx.x == 0) p.partials[(int64_t)t * p.ntiles + blockIdx.x] = s;
+  if (threadIdx.x == 0) item.partials[local] = s;
+  if (!LOOP) break;
+  __syncthreads();   // shared memory is refilled by the next tile
+  blk += gridDim.x;
+  } while (blk < list->nblocks);
 }
 
 // ---------------------------------------------------------------- aab ----
 
-template <bool FT>
+template <bool FT, bool LOOP>
 __global__ void __launch_bounds__(EPI_THREADS, 2)
-    epi_aab_kernel(const EpiArgs p) {
+    epi_aab_kernel(const EpiList *__restrict__ list) {
   extern __shared__ double sm[];
+  __shared__ EpiArgs p;
   constexpr int S = EPI_A * EPI_B * EPI_CS;
   constexpr int NIT = EPI_A * EPI_C * EPI_B / EPI_THREADS;
   // sx[a_][b_][c_] = U2[a][c][b];  sy[b_][a_][c_] = U2[b][c][a];
   // sp[a_][b_][c_] = P[c][pair(a,b)]   (R copies follow for (fT))
   double *sx = sm, *sy = sm + S, *sp = sm + 2 * S;
-
-  const int4 tl = p.tiles[blockIdx.x];
-  const int a0 = tl.x, b0 = tl.y, c0 = blockIdx.y * EPI_C;
-  const int t = blockIdx.z;
-  const int i = p.trip[3 * t], j = p.trip[3 * t + 1], k = p.trip[3 * t + 2];
+  // LOOP: a fixed grid striding over the flat tiles of all items; else one
+  // CTA per (tile, item) of a 2-D grid
+  int blk = blockIdx.x;
+  if (LOOP && blk >= list->nblocks) return;
+  do {
+  const EpiItem &item =
+      LOOP ? list->items[find_entry(list->items, list->nitems, blk,
+                                    &EpiItem::block_begin)]
+           : list->items[blockIdx.y];
+  const int local = LOOP ? blk - item.block_begin : blk;
+  if (!LOOP && local >= item.nblk) return;
+  load_args(p, item.args);
+  const int npairs = p.ntiles / p.ctiles;   // tiles: c block major
+  const int4 tl = p.tiles[local % npairs];
+  const int a0 = tl.x, b0 = tl.y, c0 = (local / npairs) * EPI_C;
+  const int i = item.i, j = item.j, k = item.k;
   const int oa = p.oa, va = p.va, ob = p.ob, vb = p.vb;
-  const double *base = p.ws + (int64_t)t * p.ws_stride;
+  const double *base = item.ws;
   const int64_t ld1 = p.ld[0], ld2 = p.ld[1], ldp = p.ld[2];
   const int64_t r1 = p.rowU1, r2 = p.rowU2;
 
@@ -267,26 +308,30 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
     if (ok_[b_]) e += (w_[b_] - x_[b_]) * r / d_[b_];
   }
   const double s = block_sum(e);
-  if (threadIdx.x == 0)
-    p.partials[(int64_t)t * p.ntiles + blockIdx.y * gridDim.x + blockIdx.x] =
-        s;
+  if (threadIdx.x == 0) item.partials[local] = s;
+  if (!LOOP) break;
+  __syncthreads();   // shared memory is refilled by the next tile
+  blk += gridDim.x;
+  } while (blk < list->nblocks);
 }
 
 __global__ void __launch_bounds__(256)
-    reduce_partials_kernel(const double *partials, int ntiles,
-                           const int *slot, double *e_slot) {
+    reduce_partials_kernel(const RedList *__restrict__ list) {
   __shared__ double red[256];
-  const int t = blockIdx.x;
-  double s = 0.0;
-  for (int x = threadIdx.x; x < ntiles; x += 256)
-    s += partials[(int64_t)t * ntiles + x];
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+  const int nitems = list->nitems;
+  for (int t = blockIdx.x; t < nitems; t += gridDim.x) {
+    const RedItem it = list->items[t];
+    double s = 0.0;
+    for (int x = threadIdx.x; x < it.n; x += 256) s += it.partials[x];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) *it.dst = red[0];
     __syncthreads();
   }
-  if (threadIdx.x == 0) e_slot[slot[t]] = red[0];
 }
 
 template <typename K>
@@ -296,6 +341,15 @@ cudaError_t set_smem(K kern, size_t bytes) {
                               (int)bytes);
 }
 
+template <typename K>
+cudaError_t launch_epi(K kern, const EpiList *d_list, size_t smem, dim3 grid,
+                       cudaStream_t st) {
+  cudaError_t e = set_smem(kern, smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, EPI_THREADS, smem, st>>>(d_list);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 size_t epi_smem_bytes(bool aab, bool ft) {
@@ -303,45 +357,62 @@ size_t epi_smem_bytes(bool aab, bool ft) {
   return (aab ? 3 : 1) * (ft ? 2 : 1) * s;
 }
 
-cudaError_t epi_aaa_launch(const EpiArgs &a, bool ft, int ntrip,
-                           cudaStream_t st) {
-  if (a.ntiles <= 0 || ntrip <= 0) return cudaSuccess;
+int epi_blocks_per_sm(bool aab, bool ft) {
+  const size_t smem = epi_smem_bytes(aab, ft);
+  int n = 0;
+  cudaError_t e;
+  if (aab) {
+    if (ft) {
+      set_smem(epi_aab_kernel<true, true>, smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, epi_aab_kernel<true, true>, EPI_THREADS, smem);
+    } else {
+      set_smem(epi_aab_kernel<false, true>, smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, epi_aab_kernel<false, true>, EPI_THREADS, smem);
+    }
+  } else {
+    if (ft) {
+      set_smem(epi_aaa_kernel<true, true>, smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, epi_aaa_kernel<true, true>, EPI_THREADS, smem);
+    } else {
+      set_smem(epi_aaa_kernel<false, true>, smem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &n, epi_aaa_kernel<false, true>, EPI_THREADS, smem);
+    }
+  }
+  return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+cudaError_t epi_aaa_launch(const EpiList *d_list, bool ft, int grid,
+                           int nitems, bool persistent, cudaStream_t st) {
+  if (grid <= 0 || nitems <= 0) return cudaSuccess;
   const size_t smem = epi_smem_bytes(false, ft);
-  dim3 grid(a.ntiles, ntrip);
-  cudaError_t e;
-  if (ft) {
-    if ((e = set_smem(epi_aaa_kernel<true>, smem)) != cudaSuccess) return e;
-    epi_aaa_kernel<true><<<grid, EPI_THREADS, smem, st>>>(a);
-  } else {
-    if ((e = set_smem(epi_aaa_kernel<false>, smem)) != cudaSuccess) return e;
-    epi_aaa_kernel<false><<<grid, EPI_THREADS, smem, st>>>(a);
-  }
-  return cudaGetLastError();
+  const dim3 g(grid, persistent ? 1 : nitems);
+  if (persistent)
+    return ft ? launch_epi(epi_aaa_kernel<true, true>, d_list, smem, g, st)
+              : launch_epi(epi_aaa_kernel<false, true>, d_list, smem, g, st);
+  return ft ? launch_epi(epi_aaa_kernel<true, false>, d_list, smem, g, st)
+            : launch_epi(epi_aaa_kernel<false, false>, d_list, smem, g, st);
 }
 
-cudaError_t epi_aab_launch(const EpiArgs &a, bool ft, int ntrip,
-                           cudaStream_t st) {
-  if (a.ntiles <= 0 || ntrip <= 0) return cudaSuccess;
+cudaError_t epi_aab_launch(const EpiList *d_list, bool ft, int grid,
+                           int nitems, bool persistent, cudaStream_t st) {
+  if (grid <= 0 || nitems <= 0) return cudaSuccess;
   const size_t smem = epi_smem_bytes(true, ft);
-  const int npairs = a.ntiles / a.ctiles;
-  dim3 grid(npairs, a.ctiles, ntrip);
-  cudaError_t e;
-  if (ft) {
-    if ((e = set_smem(epi_aab_kernel<true>, smem)) != cudaSuccess) return e;
-    epi_aab_kernel<true><<<grid, EPI_THREADS, smem, st>>>(a);
-  } else {
-    if ((e = set_smem(epi_aab_kernel<false>, smem)) != cudaSuccess) return e;
-    epi_aab_kernel<false><<<grid, EPI_THREADS, smem, st>>>(a);
-  }
-  return cudaGetLastError();
+  const dim3 g(grid, persistent ? 1 : nitems);
+  if (persistent)
+    return ft ? launch_epi(epi_aab_kernel<true, true>, d_list, smem, g, st)
+              : launch_epi(epi_aab_kernel<false, true>, d_list, smem, g, st);
+  return ft ? launch_epi(epi_aab_kernel<true, false>, d_list, smem, g, st)
+            : launch_epi(epi_aab_kernel<false, false>, d_list, smem, g, st);
 }
 
-cudaError_t reduce_partials_launch(const double *partials, int ntiles,
-                                   int ntrip, const int *slot, double *e_slot,
+cudaError_t reduce_partials_launch(const RedList *d_list, int grid,
                                    cudaStream_t st) {
-  if (ntrip <= 0) return cudaSuccess;
-  reduce_partials_kernel<<<ntrip, 256, 0, st>>>(partials, ntiles, slot,
-                                                e_slot);
+  if (grid <= 0) return cudaSuccess;
+  reduce_partials_kernel<<<grid, 256, 0, st>>>(d_list);
   return cudaGetLastError();
 }
 

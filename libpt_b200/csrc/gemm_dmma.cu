@@ -18,6 +18,13 @@
 // so the fragment loads of a half-warp read 16 consecutive doubles (no bank
 // conflicts) for both operands.
 //
+// Persistent: GEMM_GRID CTAs stride over the launch's tiles, read with the
+// jobs from a device-memory work list (GemmList), so one launch can hold the
+// triples of many plans and a captured CUDA graph can be replayed with new
+// lists.  The producer runs ahead into the next tile's operands while the
+// consumers store the current one.  Each job carries its plan's tensor maps
+// (device memory; fenced before first use).
+//
 // Tiles are numbered M-tile fastest inside a job, so the CTAs that share one
 // B (OVVV) tile run at the same time and the tile is fetched from DRAM once.
 #include "common.cuh"
@@ -35,28 +42,15 @@ constexpr uint32_t stage_bytes() {
   return (BM * BK + BK * BN) * sizeof(double);
 }
 
-__device__ __forceinline__ int find_job(const GemmJob *jobs, int njobs,
-                                        int tile) {
-  int lo = 0, hi = njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].tile_begin <= tile)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
-
 // One CTA of GEMM_THREADS (9 warps) per SM.  With 9 warps one SM
 // sub-partition hosts 3 of them, which bounds the kernel at 168 registers per
 // thread (16K registers per sub-partition); the 128-row tile's 64 FP64
 // accumulators per thread fit that without spilling.
-template <int BM>
-__global__ void __launch_bounds__(GEMM_THREADS, 1)
-    gemm_dmma_kernel(const __grid_constant__ MapSet maps,
-                     const GemmJob *__restrict__ jobs, int njobs,
-                     unsigned *err) {
+template <int BM, bool PM>
+__device__ __forceinline__ void dmma_body(const LaunchMaps *pm,
+                                          const GemmJob *__restrict__ jobs,
+                                          const int njobs, const int ntiles,
+                                          unsigned *err) {
   constexpr int MF = BM / 32;   // m16 fragments per warp (2 warp rows)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double *sA = reinterpret_cast<double *>(smem_raw);
@@ -64,12 +58,6 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
   uint64_t *full = reinterpret_cast<uint64_t *>(sB + ST * BK * BN);
   uint64_t *empty = full + ST;
 
-  const int tile = blockIdx.x;
-  const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
-  const int local = tile - job.tile_begin;
-  const int m0 = (local % job.mtiles) * BM;
-  const int n0 = (local / job.mtiles) * BN;
-  const int nseg = job.nseg;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -88,31 +76,40 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
       uint32_t phase = 0;
       int issued = 0;
       bool ok = true;
-      for (int s = 0; s < nseg && ok; ++s) {
-        const GemmSeg sg = job.seg[s];
-        const CUtensorMap *am = &maps.m[sg.amap];
-        const CUtensorMap *bm = &maps.m[sg.bmap];
-        for (int ks = 0; ks < sg.ksteps; ++ks) {
-          if (!mbar_wait(&empty[stage], phase ^ 1u, err)) {
-            ok = false;
-            break;
-          }
-          mbar_arrive_expect_tx(&full[stage], stage_bytes<BM>());
-          double *dA = sA + stage * BM * BK;
-          double *dB = sB + stage * BK * BN;
-          const int k0 = ks * BK;
+      MapSource<PM> ms(pm);
+      for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const GemmJob &job =
+            jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
+        const int local = tile - job.tile_begin;
+        const int m0 = (local % job.mtiles) * BM;
+        const int n0 = (local / job.mtiles) * BN;
+        const int nseg = job.nseg;
+        for (int s = 0; s < nseg && ok; ++s) {
+          const GemmSeg sg = job.seg[s];
+          const CUtensorMap *am = ms.get(job, sg.amap);
+          const CUtensorMap *bm = ms.get(job, sg.bmap);
+          for (int ks = 0; ks < sg.ksteps; ++ks) {
+            if (!mbar_wait(&empty[stage], phase ^ 1u, err)) {
+              ok = false;
+              break;
+            }
+            mbar_arrive_expect_tx(&full[stage], stage_bytes<BM>());
+            double *dA = sA + stage * BM * BK;
+            double *dB = sB + stage * BK * BN;
+            const int k0 = ks * BK;
 #pragma unroll
-          for (int q = 0; q < BK / 4; ++q)
-            tma_load_4d(dA + q * BM * 4, am, &full[stage], k0 + 4 * q, m0,
-                        sg.a_q, sg.a_p);
+            for (int q = 0; q < BK / 4; ++q)
+              tma_load_4d(dA + q * BM * 4, am, &full[stage], k0 + 4 * q, m0,
+                          sg.a_q, sg.a_p);
 #pragma unroll 8
-          for (int r = 0; r < BN / 4; ++r)
-            tma_load_3d(dB + r * BK * 4, bm, &full[stage], n0 + 4 * r, k0,
-                        sg.b_p);
-          ++issued;
-          if (++stage == ST) {
-            stage = 0;
-            phase ^= 1u;
+            for (int r = 0; r < BN / 4; ++r)
+              tma_load_3d(dB + r * BK * 4, bm, &full[stage], n0 + 4 * r, k0,
+                          sg.b_p);
+            ++issued;
+            if (++stage == ST) {
+              stage = 0;
+              phase ^= 1u;
+            }
           }
         }
       }
@@ -131,14 +128,6 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
   const int wn = (warp & 3) * 32;
   const int g = lane >> 2, t = lane & 3;
 
-  double acc[MF][4][4];
-#pragma unroll
-  for (int f = 0; f < MF; ++f)
-#pragma unroll
-    for (int h = 0; h < 4; ++h)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) acc[f][h][e] = 0.0;
-
   // Per-lane fragment offsets inside one stage.
   int aoff[MF];
 #pragma unroll
@@ -153,77 +142,120 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
   int stage = 0;
   uint32_t phase = 0;
   bool ok = true;
-  for (int s = 0; s < nseg && ok; ++s) {
-    const unsigned long long mask =
-        job.seg[s].neg ? 0x8000000000000000ull : 0ull;
-    const int nk = job.seg[s].ksteps;
-    for (int ks = 0; ks < nk; ++ks) {
-      if (!mbar_wait(&full[stage], phase, err)) {
-        ok = false;
-        break;
-      }
-      const double *A = sA + stage * BM * BK;
-      const double *B = sB + stage * BK * BN;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const GemmJob &job =
+        jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
+    const int local = tile - job.tile_begin;
+    const int m0 = (local % job.mtiles) * BM;
+    const int n0 = (local / job.mtiles) * BN;
+    const int nseg = job.nseg;
+
+    double acc[MF][4][4];
 #pragma unroll
-      for (int kq = 0; kq < BK / 4; ++kq) {
-        double a0[MF], a1[MF], b[4];
+    for (int f = 0; f < MF; ++f)
 #pragma unroll
-        for (int f = 0; f < MF; ++f) {
-          a0[f] = flip_sign(A[kq * BM * 4 + aoff[f]], mask);
-          a1[f] = flip_sign(A[kq * BM * 4 + aoff[f] + 32], mask);
+      for (int h = 0; h < 4; ++h)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[f][h][e] = 0.0;
+
+    for (int s = 0; s < nseg && ok; ++s) {
+      const unsigned long long mask =
+          job.seg[s].neg ? 0x8000000000000000ull : 0ull;
+      const int nk = job.seg[s].ksteps;
+      for (int ks = 0; ks < nk; ++ks) {
+        if (!mbar_wait(&full[stage], phase, err)) {
+          ok = false;
+          break;
         }
+        const double *A = sA + stage * BM * BK;
+        const double *B = sB + stage * BK * BN;
 #pragma unroll
-        for (int h = 0; h < 4; ++h) b[h] = B[kq * 16 + boff[h]];
+        for (int kq = 0; kq < BK / 4; ++kq) {
+          double a0[MF], a1[MF], b[4];
 #pragma unroll
-        for (int f = 0; f < MF; ++f)
+          for (int f = 0; f < MF; ++f) {
+            a0[f] = flip_sign(A[kq * BM * 4 + aoff[f]], mask);
+            a1[f] = flip_sign(A[kq * BM * 4 + aoff[f] + 32], mask);
+          }
 #pragma unroll
-          for (int h = 0; h < 4; ++h) dmma_16x8x4(acc[f][h], a0[f], a1[f], b[h]);
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[stage]);
-      if (++stage == ST) {
-        stage = 0;
-        phase ^= 1u;
+          for (int h = 0; h < 4; ++h) b[h] = B[kq * 16 + boff[h]];
+#pragma unroll
+          for (int f = 0; f < MF; ++f)
+#pragma unroll
+            for (int h = 0; h < 4; ++h)
+              dmma_16x8x4(acc[f][h], a0[f], a1[f], b[h]);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stage]);
+        if (++stage == ST) {
+          stage = 0;
+          phase ^= 1u;
+        }
       }
     }
-  }
-  if (!ok) return;
+    if (!ok) break;
 
-  // ---------------- store ----------------
-  double *out = job.out;
-  const int64_t ldc = job.ldc;
+    // ---------------- store ----------------
+    double *const out = job.out;
+    const int64_t ldc = job.ldc;
+    const int M = job.M, N = job.N;
 #pragma unroll
-  for (int f = 0; f < MF; ++f) {
-    const int r = m0 + wm + 16 * f + g;
+    for (int f = 0; f < MF; ++f) {
+      const int r = m0 + wm + 16 * f + g;
 #pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const int c = n0 + wn + 8 * h + 2 * t;
-      if (c < job.N) {
-        if (r < job.M)
-          *reinterpret_cast<double2 *>(out + (int64_t)r * ldc + c) =
-              make_double2(acc[f][h][0], acc[f][h][1]);
-        if (r + 8 < job.M)
-          *reinterpret_cast<double2 *>(out + (int64_t)(r + 8) * ldc + c) =
-              make_double2(acc[f][h][2], acc[f][h][3]);
+      for (int h = 0; h < 4; ++h) {
+        const int c = n0 + wn + 8 * h + 2 * t;
+        if (c < N) {
+          if (r < M)
+            *reinterpret_cast<double2 *>(out + (int64_t)r * ldc + c) =
+                make_double2(acc[f][h][0], acc[f][h][1]);
+          if (r + 8 < M)
+            *reinterpret_cast<double2 *>(out + (int64_t)(r + 8) * ldc + c) =
+                make_double2(acc[f][h][2], acc[f][h][3]);
+        }
       }
     }
   }
 }
 
 template <int BM>
-cudaError_t launch(const MapSet &maps, const GemmJob *d_jobs, int njobs,
-                   int total_tiles, unsigned *d_err, cudaStream_t st) {
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
+    gemm_dmma_kernel(const __grid_constant__ LaunchMaps pm,
+                     const GemmJob *__restrict__ jobs, int njobs, int ntiles,
+                     unsigned *err) {
+  dmma_body<BM, true>(&pm, jobs, njobs, ntiles, err);
+}
+
+template <int BM>
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
+    gemm_dmma_kernel_dm(const GemmJob *__restrict__ jobs,
+                        const GemmList *__restrict__ list, unsigned *err) {
+  dmma_body<BM, false>(nullptr, jobs, list->njobs, list->ntiles, err);
+}
+
+template <int BM>
+cudaError_t launch(const GemmJob *d_jobs, const GemmList *d_list, int njobs,
+                   int ntiles, const LaunchMaps *pm, int grid, unsigned *d_err,
+                   cudaStream_t st) {
   static bool configured = false;
   const size_t smem = gemm_smem_bytes(BM);
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(
         gemm_dmma_kernel<BM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
         (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(gemm_dmma_kernel_dm<BM>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  gemm_dmma_kernel<BM><<<total_tiles, GEMM_THREADS, smem, st>>>(
-      maps, d_jobs, njobs, d_err);
+  if (pm)
+    gemm_dmma_kernel<BM><<<grid, GEMM_THREADS, smem, st>>>(*pm, d_jobs, njobs,
+                                                           ntiles, d_err);
+  else
+    gemm_dmma_kernel_dm<BM><<<grid, GEMM_THREADS, smem, st>>>(d_jobs, d_list,
+                                                              d_err);
   return cudaGetLastError();
 }
 
@@ -234,13 +266,14 @@ size_t gemm_smem_bytes(int bm) {
          2 * ST * sizeof(uint64_t);
 }
 
-cudaError_t gemm_dmma_launch(const MapSet &maps, const GemmJob *d_jobs,
-                             int njobs, int total_tiles, int bm,
-                             unsigned *d_err, cudaStream_t st) {
-  if (total_tiles <= 0) return cudaSuccess;
+cudaError_t gemm_dmma_launch(const GemmJob *d_jobs, const GemmList *d_list,
+                             int njobs, int ntiles, const LaunchMaps *pm,
+                             int bm, int grid, unsigned *d_err,
+                             cudaStream_t st) {
+  if (grid <= 0) return cudaSuccess;
   if (bm == 96)
-    return launch<96>(maps, d_jobs, njobs, total_tiles, d_err, st);
-  return launch<128>(maps, d_jobs, njobs, total_tiles, d_err, st);
+    return launch<96>(d_jobs, d_list, njobs, ntiles, pm, grid, d_err, st);
+  return launch<128>(d_jobs, d_list, njobs, ntiles, pm, grid, d_err, st);
 }
 
 }  // namespace ptb

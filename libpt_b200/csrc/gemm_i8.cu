@@ -41,18 +41,6 @@ namespace {
 
 constexpr int BM = TC_BM;   // 128 rows (TMEM lanes)
 
-__device__ __forceinline__ int find_job(const GemmJob *jobs, int njobs,
-                                        int tile) {
-  int lo = 0, hi = njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].tile_begin <= tile)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
 
 // Shared-memory descriptor of a K-major operand stored as SW-byte swizzled
 // rows (8-row core groups SW*8 bytes apart), sm_100 descriptor version 1.
@@ -143,11 +131,11 @@ struct I8Cfg {
 constexpr int I8_THREADS = 320;   // producer, MMA issuer, 8 epilogue warps
 constexpr int I8_EPI_THREADS = 256;
 
-template <int S, int BN, int KC>
-__global__ void __launch_bounds__(I8_THREADS, 1)
-    gemm_i8_kernel(const __grid_constant__ TcMapSet maps,
-                   const GemmJob *__restrict__ jobs, int njobs,
-                   int total_tiles, unsigned *err) {
+template <int S, int BN, int KC, bool PM>
+__device__ __forceinline__ void i8_body(const LaunchMaps *pm,
+                                        const GemmJob *__restrict__ jobs,
+                                        const int njobs, const int ntiles,
+                                        unsigned *err) {
   using C = I8Cfg<S, BN, KC>;
   constexpr int ST = C::ST;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -186,14 +174,20 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
     int stage = 0;
     uint32_t phase = 0;
     bool ok = true;
-    for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
-      const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
+    MapSource<PM> ms(pm);
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+      // job fields are copied to registers: the asm memory clobbers and
+      // global stores below would otherwise force reloads
+      const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
       const int local = tile - job.tile_begin;
       const int m0 = (local % job.mtiles) * BM;
       const int n0 = (local / job.mtiles) * BN;
-      for (int s = 0; s < job.nseg && ok; ++s) {
+      const int nseg = job.nseg;
+      for (int s = 0; s < nseg && ok; ++s) {
         const GemmSeg sg = job.seg[s];
         const int aoff = sg.neg ? S : 0;
+        const CUtensorMap *am = ms.get(job, sg.amap);
+        const CUtensorMap *bm = ms.get(job, sg.bmap);
         for (int ks = 0; ks < sg.ksteps; ++ks) {
           if (!mbar_wait(&empty[stage], phase ^ 1u, err)) {
             ok = false;
@@ -207,11 +201,11 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
             for (int kk = 0; kk < C::KS; ++kk) {
               const int kc = ks * C::KS + kk;    // 32-byte K chunk
               tma_load_5d(st_base + p * C::A_TILE + kk * C::A_SUB,
-                          &maps.m[sg.amap], &full[stage], 0, m0, kc, sg.a_q,
+                          am, &full[stage], 0, m0, kc, sg.a_q,
                           p + aoff);
               tma_load_5d(st_base + S * C::A_TILE + p * C::B_TILE +
                               kk * C::B_SUB,
-                          &maps.m[sg.bmap], &full[stage], 0, n0, kc, sg.b_p, p);
+                          bm, &full[stage], 0, n0, kc, sg.b_p, p);
             }
           }
           if (++stage == ST) {
@@ -227,16 +221,17 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
     uint32_t phase = 0;
     bool ok = true;
     int it = 0;
-    for (int tile = blockIdx.x; tile < total_tiles && ok;
+    for (int tile = blockIdx.x; tile < ntiles && ok;
          tile += gridDim.x, ++it) {
-      const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
+      const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
       if (!mbar_wait(accempty, (uint32_t)((it & 1) ^ 1), err)) {
         ok = false;
         break;
       }
       tc_fence_after();
       uint32_t started = 0;   // bit w: accumulator w has been written
-      for (int s = 0; s < job.nseg && ok; ++s) {
+      const int nseg = job.nseg;
+      for (int s = 0; s < nseg && ok; ++s) {
         const int ksteps = job.seg[s].ksteps;
         for (int ks = 0; ks < ksteps; ++ks) {
           if (!mbar_wait(&full[stage], phase, err)) {
@@ -281,17 +276,19 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
     // weights of the two partial sums: hi counts units of acc_{H-1},
     // lo units of acc_{S-1}
     const double w_hi = pow2i(-7 * (H + 1)), w_lo = pow2i(-7 * (S + 1));
-    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++it) {
-      const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+      const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
       const int local = tile - job.tile_begin;
       const int m0 = (local % job.mtiles) * BM;
       const int n0 = (local / job.mtiles) * BN;
-      if (!mbar_wait(accfull, (uint32_t)(it & 1), err)) break;
-      tc_fence_after();
+      const int N = job.N;
+      const signed char *const eb = job.eb;
       const int row = m0 + 32 * q + lane;
       const bool rok = row < job.M;
-      double *orow = job.out + (int64_t)(rok ? row : 0) * job.ldc;
+      double *const orow = job.out + (int64_t)(rok ? row : 0) * job.ldc;
       const int erow = rok ? job.ea[row] : 0;
+      if (!mbar_wait(accfull, (uint32_t)(it & 1), err)) break;
+      tc_fence_after();
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
       for (int c0 = 16 * half; c0 < BN; c0 += 32) {
@@ -324,15 +321,15 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
             lo[x] = l;
           }
         }
-        if (rok && n0 + c0 < job.N) {
+        if (rok && n0 + c0 < N) {
           // the chunk's 16 column exponents in one aligned 16-byte load (the
           // exponent arrays carry 16 bytes of padding past their N entries)
-          const int4 ebv = *reinterpret_cast<const int4 *>(job.eb + n0 + c0);
+          const int4 ebv = *reinterpret_cast<const int4 *>(eb + n0 + c0);
           const signed char *eb16 = reinterpret_cast<const signed char *>(&ebv);
 #pragma unroll
           for (int x = 0; x < 16; x += 2) {
             const int col = n0 + c0 + x;
-            if (col < job.N) {
+            if (col < N) {
               // one rounding, then exact power-of-two scales
               const double v0 = fma((double)hi[x], w_hi, (double)lo[x] * w_lo) *
                                 pow2i(erow + eb16[x]);
@@ -360,20 +357,43 @@ __global__ void __launch_bounds__(I8_THREADS, 1)
 }
 
 template <int S, int BN, int KC>
-cudaError_t launch(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
-                   int total_tiles, unsigned *d_err, cudaStream_t st) {
+__global__ void __launch_bounds__(I8_THREADS, 1)
+    gemm_i8_kernel(const __grid_constant__ LaunchMaps pm,
+                   const GemmJob *__restrict__ jobs, int njobs, int ntiles,
+                   unsigned *err) {
+  i8_body<S, BN, KC, true>(&pm, jobs, njobs, ntiles, err);
+}
+
+template <int S, int BN, int KC>
+__global__ void __launch_bounds__(I8_THREADS, 1)
+    gemm_i8_kernel_dm(const GemmJob *__restrict__ jobs,
+                      const GemmList *__restrict__ list, unsigned *err) {
+  i8_body<S, BN, KC, false>(nullptr, jobs, list->njobs, list->ntiles, err);
+}
+
+template <int S, int BN, int KC>
+cudaError_t launch(const GemmJob *d_jobs, const GemmList *d_list, int njobs,
+                   int ntiles, const LaunchMaps *pm, int grid, unsigned *d_err,
+                   cudaStream_t st) {
   using C = I8Cfg<S, BN, KC>;
   static bool configured = false;
-  auto kern = gemm_i8_kernel<S, BN, KC>;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(
-        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        gemm_i8_kernel<S, BN, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        C::SMEM);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(gemm_i8_kernel_dm<S, BN, KC>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               C::SMEM);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  int grid = total_tiles < 148 ? total_tiles : 148;
-  kern<<<grid, I8_THREADS, C::SMEM, st>>>(maps, d_jobs, njobs, total_tiles,
-                                          d_err);
+  if (pm)
+    gemm_i8_kernel<S, BN, KC><<<grid, I8_THREADS, C::SMEM, st>>>(
+        *pm, d_jobs, njobs, ntiles, d_err);
+  else
+    gemm_i8_kernel_dm<S, BN, KC><<<grid, I8_THREADS, C::SMEM, st>>>(
+        d_jobs, d_list, d_err);
   return cudaGetLastError();
 }
 
@@ -395,13 +415,15 @@ int i8_tiles(int slices, const I8Tile **out) {
   }
 }
 
-cudaError_t gemm_i8_launch(int slices, I8Tile t, const TcMapSet &maps,
-                           const GemmJob *d_jobs, int njobs, int total_tiles,
-                           unsigned *d_err, cudaStream_t st) {
-  if (total_tiles <= 0) return cudaSuccess;
+cudaError_t gemm_i8_launch(int slices, I8Tile t, const GemmJob *d_jobs,
+                           const GemmList *d_list, int njobs, int ntiles,
+                           const LaunchMaps *pm, int grid, unsigned *d_err,
+                           cudaStream_t st) {
+  if (grid <= 0) return cudaSuccess;
 #define PTB_I8(S_, BN_, KC_)                                                  \
   if (slices == S_ && t.bn == BN_ && t.kc == KC_)                             \
-    return launch<S_, BN_, KC_>(maps, d_jobs, njobs, total_tiles, d_err, st);
+    return launch<S_, BN_, KC_>(d_jobs, d_list, njobs, ntiles, pm, grid,     \
+                                d_err, st);
   PTB_I8(4, 128, 32) PTB_I8(4, 128, 64) PTB_I8(4, 64, 32) PTB_I8(4, 64, 64)
   PTB_I8(5, 96, 32) PTB_I8(5, 96, 64) PTB_I8(5, 64, 32) PTB_I8(5, 64, 64)
   PTB_I8(6, 80, 32) PTB_I8(6, 64, 32) PTB_I8(6, 64, 64)

@@ -28,18 +28,6 @@ namespace {
 
 constexpr int BM = TC_BM;   // 128 rows (TMEM lanes)
 
-__device__ __forceinline__ int find_job(const GemmJob *jobs, int njobs,
-                                        int tile) {
-  int lo = 0, hi = njobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (jobs[mid].tile_begin <= tile)
-      lo = mid;
-    else
-      hi = mid - 1;
-  }
-  return lo;
-}
 
 // Shared-memory matrix descriptor of a K-major operand stored as SW-byte
 // swizzled rows (8-row core groups SW*8 bytes apart), sm_100 version 1.
@@ -119,12 +107,13 @@ struct TcCfg {
   static_assert(STAGE % 1024 == 0, "stage tiles keep 1 KiB alignment");
 };
 
-template <int KIND, int BN, int NPL, int NACC, int ST, int SW, int NBUF>
-__global__ void __launch_bounds__(192, 1)
-    gemm_tc_kernel(const __grid_constant__ TcMapSet maps,
-                   const GemmJob *__restrict__ jobs, int njobs,
-                   int total_tiles, const __grid_constant__ TcProducts prods,
-                   unsigned *err) {
+template <int KIND, int BN, int NPL, int NACC, int ST, int SW, int NBUF,
+          bool PM>
+__device__ __forceinline__ void tc_body(const LaunchMaps *pm,
+                                        const GemmJob *__restrict__ jobs,
+                                        const int njobs, const int ntiles,
+                                        const TcProducts &prods,
+                                        unsigned *err) {
   using C = TcCfg<KIND, BN, NPL, NACC, ST, SW, NBUF>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -164,13 +153,16 @@ __global__ void __launch_bounds__(192, 1)
     int stage = 0;
     uint32_t phase = 0;
     bool ok = true;
-    for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
-      const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
+    MapSource<PM> ms(pm);
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+      const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
       const int local = tile - job.tile_begin;
       const int m0 = (local % job.mtiles) * BM;
       const int n0 = (local / job.mtiles) * BN;
-      for (int s = 0; s < job.nseg && ok; ++s) {
+      const int nseg = job.nseg;
+      for (int s = 0; s < nseg && ok; ++s) {
         const GemmSeg sg = job.seg[s];
+
         for (int ks = 0; ks < sg.ksteps; ++ks) {
           if (!mbar_wait(&empty[stage], phase ^ 1u, err)) {
             ok = false;
@@ -181,10 +173,11 @@ __global__ void __launch_bounds__(192, 1)
           const int k0 = ks * C::KELEM;
 #pragma unroll
           for (int p = 0; p < NPL; ++p) {
-            tma_load_4d(st_base + p * C::A_TILE, &maps.m[sg.amap + p],
+            tma_load_4d(st_base + p * C::A_TILE, ms.get(job, sg.amap + p),
                         &full[stage], k0, m0, sg.a_q, sg.a_p);
             tma_load_3d(st_base + NPL * C::A_TILE + p * C::B_TILE,
-                        &maps.m[sg.bmap + p], &full[stage], k0, n0, sg.b_p);
+                        ms.get(job, sg.bmap + p), &full[stage], k0, n0,
+                        sg.b_p);
           }
           if (++stage == ST) {
             stage = 0;
@@ -199,9 +192,9 @@ __global__ void __launch_bounds__(192, 1)
     uint32_t phase = 0;
     bool ok = true;
     int it = 0;
-    for (int tile = blockIdx.x; tile < total_tiles && ok;
+    for (int tile = blockIdx.x; tile < ntiles && ok;
          tile += gridDim.x, ++it) {
-      const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
+      const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
       const int ab = NBUF == 2 ? (it & 1) : 0;
       const uint32_t epar = NBUF == 2 ? (uint32_t)(((it >> 1) & 1) ^ 1)
                                       : (uint32_t)((it & 1) ^ 1);
@@ -212,7 +205,8 @@ __global__ void __launch_bounds__(192, 1)
       tc_fence_after();
       const uint32_t acc0 = tmem + (uint32_t)(ab * NACC * BN);
       uint32_t started = 0;   // bit c: accumulator c has been written
-      for (int s = 0; s < job.nseg && ok; ++s) {
+      const int nseg = job.nseg;
+      for (int s = 0; s < nseg && ok; ++s) {
         const GemmSeg sg = job.seg[s];
         const uint32_t neg = sg.neg ? (1u << 13) : 0u;   // negate A
         for (int ks = 0; ks < sg.ksteps; ++ks) {
@@ -250,8 +244,8 @@ __global__ void __launch_bounds__(192, 1)
     // ---------------- epilogue ----------------
     const int q = warp & 3;            // TMEM lane quarter of this warp
     int it = 0;
-    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++it) {
-      const GemmJob &job = jobs[find_job(jobs, njobs, tile)];
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+      const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
       const int local = tile - job.tile_begin;
       const int m0 = (local % job.mtiles) * BM;
       const int n0 = (local / job.mtiles) * BN;
@@ -260,8 +254,11 @@ __global__ void __launch_bounds__(192, 1)
                                       : (uint32_t)(it & 1);
       if (!mbar_wait(&accfull[ab], fpar, err)) break;
       tc_fence_after();
+      // job fields in registers (stores and asm clobbers force reloads)
       const int row = m0 + 32 * q + lane;
-      double *orow = job.out + (int64_t)row * job.ldc;
+      const int N = job.N;
+      const bool rok = row < job.M;
+      double *const orow = job.out + (int64_t)(rok ? row : 0) * job.ldc;
       const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16) +
                              (uint32_t)(ab * NACC * BN);
 #pragma unroll 1
@@ -272,11 +269,11 @@ __global__ void __launch_bounds__(192, 1)
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
         for (int x = 0; x < 32; ++x) v[x] = (double)__uint_as_float(r[x]);
-        if (row < job.M) {
+        if (rok) {
 #pragma unroll
           for (int x = 0; x < 32; x += 2) {
             const int col = n0 + c0 + x;
-            if (col < job.N) {
+            if (col < N) {
               *reinterpret_cast<double2 *>(orow + col) =
                   make_double2(v[x], v[x + 1]);
             }
@@ -299,21 +296,44 @@ __global__ void __launch_bounds__(192, 1)
 }
 
 template <int KIND, int BN, int NPL, int NACC, int ST, int SW, int NBUF>
-cudaError_t launch(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
-                   int total_tiles, const TcProducts &prods, unsigned *d_err,
-                   cudaStream_t st) {
+__global__ void __launch_bounds__(192, 1)
+    gemm_tc_kernel(const __grid_constant__ LaunchMaps pm,
+                   const GemmJob *__restrict__ jobs, int njobs, int ntiles,
+                   const __grid_constant__ TcProducts prods, unsigned *err) {
+  tc_body<KIND, BN, NPL, NACC, ST, SW, NBUF, true>(&pm, jobs, njobs, ntiles,
+                                                   prods, err);
+}
+
+template <int KIND, int BN, int NPL, int NACC, int ST, int SW, int NBUF>
+__global__ void __launch_bounds__(192, 1)
+    gemm_tc_kernel_dm(const GemmJob *__restrict__ jobs,
+                      const GemmList *__restrict__ list,
+                      const __grid_constant__ TcProducts prods, unsigned *err) {
+  tc_body<KIND, BN, NPL, NACC, ST, SW, NBUF, false>(
+      nullptr, jobs, list->njobs, list->ntiles, prods, err);
+}
+
+template <int KIND, int BN, int NPL, int NACC, int ST, int SW, int NBUF>
+cudaError_t launch(const GemmJob *d_jobs, const GemmList *d_list, int njobs,
+                   int ntiles, const LaunchMaps *pm, int grid,
+                   const TcProducts &prods, unsigned *d_err, cudaStream_t st) {
   using C = TcCfg<KIND, BN, NPL, NACC, ST, SW, NBUF>;
   static bool configured = false;
-  auto kern = gemm_tc_kernel<KIND, BN, NPL, NACC, ST, SW, NBUF>;
+  auto kp = gemm_tc_kernel<KIND, BN, NPL, NACC, ST, SW, NBUF>;
+  auto kd = gemm_tc_kernel_dm<KIND, BN, NPL, NACC, ST, SW, NBUF>;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(
-        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        kp, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(kd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               C::SMEM);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  int grid = total_tiles < 148 ? total_tiles : 148;
-  kern<<<grid, 192, C::SMEM, st>>>(maps, d_jobs, njobs, total_tiles, prods,
-                                   d_err);
+  if (pm)
+    kp<<<grid, 192, C::SMEM, st>>>(*pm, d_jobs, njobs, ntiles, prods, d_err);
+  else
+    kd<<<grid, 192, C::SMEM, st>>>(d_jobs, d_list, prods, d_err);
   return cudaGetLastError();
 }
 
@@ -321,15 +341,13 @@ cudaError_t launch(const TcMapSet &maps, const GemmJob *d_jobs, int njobs,
 
 int tc_kchunk_elems(int kind) { return kind == TC_TF32 ? 32 : 0; }
 
-cudaError_t gemm_tc_launch(int kind, const TcMapSet &maps,
-                           const GemmJob *d_jobs, int njobs, int total_tiles,
-                           const TcProducts &prods, unsigned *d_err,
-                           cudaStream_t st, int slices) {
-  (void)slices;
-  if (total_tiles <= 0) return cudaSuccess;
-  if (kind != TC_TF32) return cudaErrorInvalidValue;
-  return launch<TC_TF32, TC_BN, 2, 1, 2, 128, 2>(maps, d_jobs, njobs,
-                                                 total_tiles, prods, d_err, st);
+cudaError_t gemm_tc_launch(const GemmJob *d_jobs, const GemmList *d_list,
+                           int njobs, int ntiles, const LaunchMaps *pm,
+                           int grid, const TcProducts &prods, unsigned *d_err,
+                           cudaStream_t st) {
+  if (grid <= 0) return cudaSuccess;
+  return launch<TC_TF32, TC_BN, 2, 1, 2, 128, 2>(d_jobs, d_list, njobs, ntiles,
+                                                 pm, grid, prods, d_err, st);
 }
 
 }  // namespace ptb

@@ -36,15 +36,6 @@ int64_t pad32(int64_t x) { return (x + 31) & ~int64_t(31); }
 int64_t npair(int64_t v) { return v * (v - 1) / 2; }
 int ksteps(int64_t k) { return (int)((k + GEMM_BK - 1) / GEMM_BK); }
 
-#define CK(call)                                                          \
-  do {                                                                    \
-    cudaError_t e_ = (call);                                              \
-    if (e_ != cudaSuccess) {                                              \
-      set_error(std::string(#call) + ": " + cudaGetErrorString(e_));      \
-      return e_ == cudaErrorMemoryAllocation ? LIBPT_ERR_NOMEM            \
-                                             : LIBPT_ERR_CUDA;            \
-    }                                                                     \
-  } while (0)
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType,
                                   cuuint32_t, void *, const cuuint64_t *,
@@ -570,7 +561,7 @@ int build_aaa(libpt_plan *p, SpinCase &c) {
   }
   EpiArgs &e = c.epi;
   memset(&e, 0, sizeof(e));
-  e.ws_stride = stride;
+  c.ws_stride = stride;
   e.offL[0] = offs[0];
   e.offR[0] = p->ft ? offs[1] : -1;
   e.ld[0] = ldT;
@@ -605,6 +596,9 @@ int build_aaa(libpt_plan *p, SpinCase &c) {
                        cudaMemcpyHostToDevice, p->st));
     CK(cudaStreamSynchronize(p->st));
   }
+  e.ntiles = c.ntiles;
+  e.tiles = c.d_tiles;
+  e.ctiles = c.ctiles;
   const double vv = (double)v;
   c.flops_per_triple = 3.0 * vv * vv * vv * (vv - 1) + 6.0 * o * vv * vv * vv;
   if (p->ft) c.flops_per_triple *= 2;
@@ -686,7 +680,7 @@ int build_aab(libpt_plan *p, SpinCase &c) {
   }
   EpiArgs &e = c.epi;
   memset(&e, 0, sizeof(e));
-  e.ws_stride = stride;
+  c.ws_stride = stride;
   for (int q = 0; q < 3; ++q) {
     e.offL[q] = offs[0][q];
     e.offR[q] = p->ft ? offs[1][q] : -1;
@@ -731,6 +725,9 @@ int build_aab(libpt_plan *p, SpinCase &c) {
                        cudaMemcpyHostToDevice, p->st));
     CK(cudaStreamSynchronize(p->st));
   }
+  e.ntiles = c.ntiles;
+  e.tiles = c.d_tiles;
+  e.ctiles = c.ctiles;
   const double A = (double)va, B = (double)vb;
   c.flops_per_triple = 2 * A * A * A * B + 4 * A * A * B * B +
                        2 * B * A * A * (A - 1) + 6 * A * A * B * oa +
@@ -928,149 +925,199 @@ int add_cases(libpt_plan *p) {
   return LIBPT_OK;
 }
 
-// Runs queue entries of one case, `n` at a time.
-int run_case(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents) {
-  const size_t per = (size_t)c.epi.ws_stride * sizeof(double);
-  size_t nb = p->ws_budget / std::max<size_t>(per, 1);
-  if (p->max_batch) nb = std::min(nb, p->max_batch);
-  nb = std::max<size_t>(1, std::min<size_t>({nb, (size_t)4096, ents.size()}));
-  if (nb * per > p->ws_bytes) {
-    if (p->ws) {
-      cudaFree(p->ws);
-      p->allocs.erase(std::find(p->allocs.begin(), p->allocs.end(), (void *)p->ws));
-      p->ws = nullptr;
-    }
-    if (dalloc(p, (void **)&p->ws, nb * per)) return LIBPT_ERR_NOMEM;
-    p->ws_bytes = nb * per;
+// Copies each case's kernel views (tensor maps) and epilogue arguments to
+// device memory, where the kernels read them.  Re-run after any map change.
+int upload_views(libpt_plan *p) {
+  for (SpinCase &c : p->cases) {
+    if (!c.count) continue;
+    const size_t mb = sizeof(TcMapSet);   // >= sizeof(MapSet)
+    if (!c.d_maps && dalloc(p, (void **)&c.d_maps, mb)) return LIBPT_ERR_NOMEM;
+    if (!c.d_epi && dalloc(p, (void **)&c.d_epi, sizeof(EpiArgs)))
+      return LIBPT_ERR_NOMEM;
+    const void *src = p->precision == LIBPT_PREC_FP64
+                          ? (const void *)&c.maps
+                          : (const void *)&c.tcmaps;
+    const size_t n = p->precision == LIBPT_PREC_FP64 ? sizeof(MapSet)
+                                                     : sizeof(TcMapSet);
+    CK(cudaMemcpyAsync(c.d_maps, src, n, cudaMemcpyHostToDevice, p->st));
+    CK(cudaMemcpyAsync(c.d_epi, &c.epi, sizeof(EpiArgs),
+                       cudaMemcpyHostToDevice, p->st));
   }
-  const size_t njt = c.jobs.size();
-  std::vector<GemmJob> jobs;
-  std::vector<int> trip, slot;
-  for (size_t b0 = 0; b0 < ents.size(); b0 += nb) {
-    const size_t n = std::min(nb, ents.size() - b0);
-    // buffers sized for this batch
-    if (n * njt > p->jobs_cap) {
-      if (dalloc(p, (void **)&p->d_jobs, n * njt * sizeof(GemmJob))) return LIBPT_ERR_NOMEM;
-      p->jobs_cap = n * njt;
-    }
-    if (n > p->trip_cap) {
-      if (dalloc(p, (void **)&p->d_trip, 3 * n * sizeof(int))) return LIBPT_ERR_NOMEM;
-      if (dalloc(p, (void **)&p->d_slot, n * sizeof(int))) return LIBPT_ERR_NOMEM;
-      p->trip_cap = n;
-    }
-    if (n * (size_t)c.ntiles > p->partials_cap) {
-      if (dalloc(p, (void **)&p->partials, n * c.ntiles * sizeof(double)))
-        return LIBPT_ERR_NOMEM;
-      p->partials_cap = n * c.ntiles;
-    }
-    jobs.clear();
-    trip.clear();
-    slot.clear();
-    int tiles = 0;
-    for (size_t t = 0; t < n; ++t) {
-      const int4 q = p->queue[ents[b0 + t]];
-      const int ijk[3] = {q.y, q.z, q.w};
-      trip.push_back(q.y);
-      trip.push_back(q.z);
-      trip.push_back(q.w);
-      slot.push_back((int)ents[b0 + t]);
-      for (const JobT &jt : c.jobs) {
-        GemmJob g;
-        memset(&g, 0, sizeof(g));
-        g.out = p->ws + (int64_t)t * c.epi.ws_stride + jt.off;
-        g.ldc = jt.ldc;
-        g.M = jt.M;
-        g.N = jt.N;
-        const bool tc = p->precision == LIBPT_PREC_TF32X3;
-        const bool i8 = p->precision == LIBPT_PREC_EMU64;
-        const int bn = tc ? TC_BN : i8 ? p->i8tile.bn : GEMM_BN;
-        const int bmr = (tc || i8) ? TC_BM : c.bm;
-        g.ea = jt.ea;
-        g.eb = jt.eb;
-        g.ntiles_n = (jt.N + bn - 1) / bn;
-        g.mtiles = (jt.M + bmr - 1) / bmr;
-        g.tile_begin = tiles;
-        g.nseg = jt.nseg;
-        for (int s = 0; s < jt.nseg; ++s) {
-          const SegT &st = jt.seg[s];
-          GemmSeg &gs = g.seg[s];
-          gs.amap = (int16_t)(tc ? 2 * st.amap : st.amap);
-          gs.bmap = (int16_t)(tc ? 2 * st.bmap : st.bmap);
-          gs.neg = st.neg;
-          gs.a_q = ijk[st.aq];
-          gs.a_p = ijk[st.ap];
-          if (i8) {   // INT8 A views merge (Q, P) into one coordinate
-            gs.a_q = gs.a_p * (int32_t)c.opd[st.amap].Q + gs.a_q;
-            gs.a_p = 0;
-          }
-          gs.b_p = ijk[st.bp];
-          gs.ksteps = tc ? (st.k + tc_kchunk_elems(TC_TF32) - 1) /
-                               tc_kchunk_elems(TC_TF32)
-                    : i8 ? (st.k + p->i8tile.kc - 1) / p->i8tile.kc
-                         : st.ksteps;
+  // the sources are members of the plan, copied before they can change
+  CK(cudaStreamSynchronize(p->st));
+  return LIBPT_OK;
+}
+
+// Sizes the round resources for `ents` (up to the workspace budget): the
+// contraction outputs of every triple, their partial energies and the
+// round descriptors.
+int ensure_capacity(libpt_plan *p, const std::vector<int64_t> &ents) {
+  int64_t want = 0, biggest = 0;
+  for (int64_t q : ents) {
+    const int64_t st = p->cases[p->queue[q].x].ws_stride;
+    want += st;
+    biggest = std::max(biggest, st);
+    if (want * 8 >= (int64_t)p->ws_budget) break;
+  }
+  want = std::max(std::min<int64_t>(want, (int64_t)(p->ws_budget / 8)), biggest);
+  const size_t tri = std::max<size_t>(
+      1, std::min<size_t>({(size_t)4096, ents.size(),
+                           (size_t)(want / std::max<int64_t>(p->ws_stride_min, 1))}));
+  if (want <= p->ws_cap && tri <= p->tri_cap) return LIBPT_OK;
+  if (p->arena) {
+    set_error("scratch arena workspace exceeded");
+    return LIBPT_ERR_NOMEM;
+  }
+  CK(cudaStreamSynchronize(p->st));
+  for (void **q : {(void **)&p->ws, (void **)&p->partials, (void **)&p->d_desc}) {
+    if (!*q) continue;
+    auto it = std::find(p->allocs.begin(), p->allocs.end(), *q);
+    if (it != p->allocs.end()) p->allocs.erase(it);
+    cudaFree(*q);
+    *q = nullptr;
+  }
+  if (p->exec_ready) {
+    p->exec.destroy();
+    p->exec_ready = false;
+  }
+  p->ws_cap = p->part_cap = 0;
+  p->tri_cap = 0;
+  const int64_t part = (int64_t)tri * std::max(p->ntiles_max, 1);
+  const size_t desc = Executor::bytes_for(tri, p->jobs_max);
+  if (dalloc(p, (void **)&p->ws, want * 8) ||
+      dalloc(p, (void **)&p->partials, part * 8) ||
+      dalloc(p, (void **)&p->d_desc, desc))
+    return LIBPT_ERR_NOMEM;
+  if (int r = p->exec.init(p->st, p->d_desc, desc, false)) return r;
+  p->exec_ready = true;
+  p->ws_cap = want;
+  p->part_cap = part;
+  p->tri_cap = tri;
+  return LIBPT_OK;
+}
+
+}  // namespace
+
+GemmGroup plan_group(const libpt_plan *p, const SpinCase &c) {
+  GemmGroup g;
+  if (p->precision == LIBPT_PREC_EMU64) {
+    g.kind = 2;
+    g.bm = TC_BM;
+    g.slices = p->slices;
+    g.tile = p->i8tile;
+  } else if (p->precision == LIBPT_PREC_TF32X3) {
+    g.kind = 1;
+    g.bm = TC_BM;
+  } else {
+    g.kind = 0;
+    g.bm = c.bm;
+  }
+  return g;
+}
+
+int plan_append(libpt_plan *p, const int64_t *ents, size_t n, PlanCursor &cur,
+                Round &r, size_t *taken) {
+  *taken = 0;
+  const bool tc = p->precision == LIBPT_PREC_TF32X3;
+  const bool i8 = p->precision == LIBPT_PREC_EMU64;
+  for (size_t t = 0; t < n; ++t) {
+    const int4 q = p->queue[ents[t]];
+    SpinCase &c = p->cases[q.x];
+    if (cur.triples >= p->tri_cap || cur.ws + c.ws_stride > p->ws_cap ||
+        cur.part + c.ntiles > p->part_cap)
+      break;   // the round is full for this plan
+    const int ijk[3] = {q.y, q.z, q.w};
+    double *ws = p->ws + cur.ws;
+    double *partials = p->partials + cur.part;
+    cur.ws += c.ws_stride;
+    cur.part += c.ntiles;
+    ++cur.triples;
+    ++*taken;
+    const GemmGroup grp = plan_group(p, c);
+    std::vector<GemmJob> &jobs = r.gemm[grp];
+    const CUtensorMap *hmaps = p->precision == LIBPT_PREC_FP64 ? c.maps.m
+                                                               : c.tcmaps.m;
+    const int map0 = r.maps[grp].add(c.d_maps, hmaps, tc ? TC_MAX_MAPS : MAX_MAPS);
+    const int bn = tc ? TC_BN : i8 ? p->i8tile.bn : GEMM_BN;
+    const int bmr = (tc || i8) ? TC_BM : c.bm;
+    for (const JobT &jt : c.jobs) {
+      GemmJob g;
+      memset(&g, 0, sizeof(g));
+      g.out = ws + jt.off;
+      g.ldc = jt.ldc;
+      g.M = jt.M;
+      g.N = jt.N;
+      g.ea = jt.ea;
+      g.eb = jt.eb;
+      g.maps = c.d_maps;
+      g.map0 = map0;
+      g.ntiles_n = (jt.N + bn - 1) / bn;
+      g.mtiles = (jt.M + bmr - 1) / bmr;
+      g.nseg = jt.nseg;
+      for (int s = 0; s < jt.nseg; ++s) {
+        const SegT &st = jt.seg[s];
+        GemmSeg &gs = g.seg[s];
+        gs.amap = (int16_t)(tc ? 2 * st.amap : st.amap);
+        gs.bmap = (int16_t)(tc ? 2 * st.bmap : st.bmap);
+        gs.neg = st.neg;
+        gs.a_q = ijk[st.aq];
+        gs.a_p = ijk[st.ap];
+        if (i8) {   // INT8 A views merge (Q, P) into one coordinate
+          gs.a_q = gs.a_p * (int32_t)c.opd[st.amap].Q + gs.a_q;
+          gs.a_p = 0;
         }
-        tiles += g.mtiles * g.ntiles_n;
-        jobs.push_back(g);
+        gs.b_p = ijk[st.bp];
+        gs.ksteps = tc ? (st.k + tc_kchunk_elems(TC_TF32) - 1) /
+                             tc_kchunk_elems(TC_TF32)
+                  : i8 ? (st.k + p->i8tile.kc - 1) / p->i8tile.kc
+                       : st.ksteps;
       }
+      jobs.push_back(g);
     }
-    CK(cudaMemcpyAsync(p->d_jobs, jobs.data(), jobs.size() * sizeof(GemmJob),
-                       cudaMemcpyHostToDevice, p->st));
-    CK(cudaMemcpyAsync(p->d_trip, trip.data(), trip.size() * sizeof(int),
-                       cudaMemcpyHostToDevice, p->st));
-    CK(cudaMemcpyAsync(p->d_slot, slot.data(), slot.size() * sizeof(int),
-                       cudaMemcpyHostToDevice, p->st));
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    if (p->timing) {
-      for (int x = 0; x < 4; ++x) CK(cudaEventCreate(&ev[x]));
-      CK(cudaEventRecord(ev[0], p->st));
+    EpiItem e;
+    memset(&e, 0, sizeof(e));
+    e.args = c.d_epi;
+    e.ws = ws;
+    e.partials = partials;
+    e.i = q.y;
+    e.j = q.z;
+    e.k = q.w;
+    r.epi[c.type][p->ft ? 1 : 0].push_back(e);
+    r.epi_blocks[c.type][p->ft ? 1 : 0].push_back(c.ntiles);
+    RedItem red;
+    red.partials = e.partials;
+    red.dst = p->e_slot + ents[t];
+    red.n = c.ntiles;
+    red.pad_ = 0;
+    r.red.push_back(red);
+    r.gemm_flops += c.flops_per_triple;
+    ++r.triples;
+  }
+  return LIBPT_OK;
+}
+
+namespace {
+
+// Runs queue entries in rounds, each filling the plan's round resources.
+int run_entries(libpt_plan *p, const std::vector<int64_t> &ents) {
+  if (ents.empty()) return LIBPT_OK;
+  if (int r = ensure_capacity(p, ents)) return r;
+  Round round;
+  for (size_t b0 = 0; b0 < ents.size();) {
+    round.clear();
+    PlanCursor cur;
+    size_t taken = 0;
+    if (int r = plan_append(p, ents.data() + b0, ents.size() - b0, cur, round,
+                            &taken))
+      return r;
+    if (taken == 0) {
+      set_error("a triple does not fit the round resources");
+      return LIBPT_ERR_NOMEM;
     }
-    if (p->precision == LIBPT_PREC_EMU64) {
-      CK(gemm_i8_launch(p->slices, p->i8tile, c.tcmaps, p->d_jobs,
-                        (int)jobs.size(), tiles, p->d_err, p->st));
-    } else if (p->precision == LIBPT_PREC_TF32X3) {
-      TcProducts pr;
-      memset(&pr, 0, sizeof(pr));
-      const int8_t pa[3] = {0, 0, 1}, pb[3] = {0, 1, 0};   // hh + hl + lh
-      for (int q = 0; q < 3; ++q) {
-        pr.pa[q] = pa[q];
-        pr.pb[q] = pb[q];
-        pr.acc[q] = 0;
-      }
-      pr.n = 3;
-      CK(gemm_tc_launch(TC_TF32, c.tcmaps, p->d_jobs, (int)jobs.size(), tiles,
-                        pr, p->d_err, p->st));
-    } else {
-      CK(gemm_dmma_launch(c.maps, p->d_jobs, (int)jobs.size(), tiles, c.bm,
-                          p->d_err, p->st));
-    }
-    if (p->timing) {
-      CK(cudaEventRecord(ev[1], p->st));
-      CK(cudaEventRecord(ev[2], p->st));
-    }
-    p->launches += (tiles > 0) + (c.ntiles > 0) + 1;
-    EpiArgs e = c.epi;
-    e.ws = p->ws;
-    e.trip = p->d_trip;
-    e.partials = p->partials;
-    e.ntiles = c.ntiles;
-    e.tiles = c.d_tiles;
-    e.ctiles = c.ctiles;
-    if (c.type == 0)
-      CK(epi_aaa_launch(e, p->ft, (int)n, p->st));
-    else
-      CK(epi_aab_launch(e, p->ft, (int)n, p->st));
-    if (p->timing) {
-      CK(cudaEventRecord(ev[3], p->st));
-      p->ev_gemm.push_back(ev[0]);
-      p->ev_gemm.push_back(ev[1]);
-      p->ev_epi.push_back(ev[2]);
-      p->ev_epi.push_back(ev[3]);
-      double fl = 0.0;
-      for (size_t t = 0; t < n; ++t) fl += c.flops_per_triple;
-      p->flops_gemm.push_back(fl);
-    }
-    CK(reduce_partials_launch(p->partials, c.ntiles, (int)n, p->d_slot,
-                              p->e_slot, p->st));
+    b0 += taken;
+    if (int r = p->exec.run(round, p->d_err, p->timing ? &p->tm : nullptr,
+                            &p->launches))
+      return r;
   }
   return LIBPT_OK;
 }
@@ -1083,7 +1130,7 @@ int probe_ms(libpt_plan *p, SpinCase &c, const std::vector<int64_t> &ents,
   CK(cudaEventCreate(&e1));
   int r = LIBPT_OK;
   CK(cudaEventRecord(e0, p->st));
-  r = run_case(p, c, ents);
+  r = run_entries(p, ents);
   if (!r) {
     CK(cudaEventRecord(e1, p->st));
     CK(cudaEventSynchronize(e1));
@@ -1132,7 +1179,7 @@ int autotune(libpt_plan *p) {
         if (p->cases[ci].count && (choice[ci] == 96 || choice[ci] == 128))
           if (int r = set_bm(p->cases[ci], choice[ci])) return r;
     }
-    return LIBPT_OK;
+    return upload_views(p);
   }
   if (!tune_enabled()) return LIBPT_OK;
   // probe: the first triples of the case with the most work
@@ -1160,6 +1207,7 @@ int autotune(libpt_plan *p) {
     for (int t = 0; t < ntiles && !r; ++t) {
       p->i8tile = tiles[t];
       r = i8_encode(p, p->cases[big]);
+      if (!r) r = upload_views(p);
       float ms = 0.f;
       if (!r) r = probe_ms(p, p->cases[big], ents, &ms);
       if (!r) r = probe_ms(p, p->cases[big], ents, &ms);
@@ -1176,6 +1224,7 @@ int autotune(libpt_plan *p) {
     for (SpinCase &c : p->cases)
       if (c.count)
         if ((r = i8_encode(p, c))) return r;
+    if ((r = upload_views(p))) return r;
     choice.assign(1, best);
   } else {
     choice.assign(p->cases.size(), 0);
@@ -1188,6 +1237,7 @@ int autotune(libpt_plan *p) {
       float best_ms = 0.f;
       for (int bm : {start, start == 96 ? 128 : 96}) {
         if ((r = set_bm(c, bm))) break;
+        if ((r = upload_views(p))) break;
         float ms = 0.f;
         if ((r = probe_ms(p, c, ents, &ms))) break;
         if ((r = probe_ms(p, c, ents, &ms))) break;
@@ -1200,6 +1250,7 @@ int autotune(libpt_plan *p) {
         }
       }
       if (!r) r = set_bm(c, best);
+      if (!r) r = upload_views(p);
       choice[ci] = best;
     }
     if (r) return r;
@@ -1345,22 +1396,28 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       r = LIBPT_ERR_CUDA;
       break;
     }
+    // round geometry: the largest and smallest triples of the cases
+    for (const SpinCase &c : p->cases)
+      if (c.count) {
+        p->ws_stride = std::max<int64_t>(p->ws_stride, c.ws_stride);
+        p->ws_stride_min = p->ws_stride_min
+                               ? std::min<int64_t>(p->ws_stride_min, c.ws_stride)
+                               : c.ws_stride;
+        p->ntiles_max = std::max(p->ntiles_max, c.ntiles);
+        p->jobs_max = std::max(p->jobs_max, c.jobs.size());
+      }
+    if ((r = upload_views(p))) break;
+    if (p->queue.empty()) break;
     if (p->arena) {
       // arena: size the batch buffers once, from what the arena has left
-      int64_t stride = 0, ntl = 0;
-      size_t njt = 0;
-      for (const SpinCase &c : p->cases)
-        if (c.count) {
-          stride = std::max<int64_t>(stride, c.epi.ws_stride);
-          ntl = std::max<int64_t>(ntl, c.ntiles);
-          njt = std::max(njt, c.jobs.size());
-        }
-      if (p->queue.empty()) break;
-      const size_t per = (size_t)stride * 8 + (size_t)ntl * 8 +
-                         njt * sizeof(GemmJob) + 16;
+      const size_t d0 = Executor::bytes_for(0, p->jobs_max);
+      const size_t per = (size_t)p->ws_stride * 8 +
+                         (size_t)std::max(p->ntiles_max, 1) * 8 +
+                         (Executor::bytes_for(1, p->jobs_max) - d0);
       const size_t used = (p->arena_used + 255) & ~size_t(255);
+      const size_t slack = 3 * 256 + d0;
       const size_t left =
-          p->arena_size > used + 5 * 256 ? p->arena_size - used - 5 * 256 : 0;
+          p->arena_size > used + slack ? p->arena_size - used - slack : 0;
       const size_t nb = std::min<size_t>({left / per, (size_t)4096,
                                           p->queue.size()});
       if (nb == 0) {
@@ -1368,20 +1425,22 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
         r = LIBPT_ERR_NOMEM;
         break;
       }
-      if ((r = dalloc(p, (void **)&p->ws, nb * stride * 8))) break;
-      if ((r = dalloc(p, (void **)&p->partials, nb * ntl * 8))) break;
-      if ((r = dalloc(p, (void **)&p->d_jobs, nb * njt * sizeof(GemmJob)))) break;
-      if ((r = dalloc(p, (void **)&p->d_trip, 3 * nb * sizeof(int)))) break;
-      if ((r = dalloc(p, (void **)&p->d_slot, nb * sizeof(int)))) break;
-      p->ws_bytes = p->ws_budget = nb * stride * 8;
-      p->partials_cap = nb * ntl;
-      p->jobs_cap = nb * njt;
-      p->trip_cap = nb;
-      p->max_batch = nb;
+      const size_t desc = Executor::bytes_for(nb, p->jobs_max);
+      if ((r = dalloc(p, (void **)&p->ws, nb * p->ws_stride * 8))) break;
+      if ((r = dalloc(p, (void **)&p->partials,
+                      nb * std::max(p->ntiles_max, 1) * 8)))
+        break;
+      if ((r = dalloc(p, (void **)&p->d_desc, desc))) break;
+      if ((r = p->exec.init(st, p->d_desc, desc, false))) break;
+      p->exec_ready = true;
+      p->ws_cap = (int64_t)nb * p->ws_stride;
+      p->part_cap = (int64_t)nb * std::max(p->ntiles_max, 1);
+      p->tri_cap = p->max_batch = nb;
+      p->ws_budget = nb * p->ws_stride * 8;
       break;
     }
     // workspace budget: half of what is free, between 64 MiB and 16 GiB;
-    // the buffer itself is allocated by the first batch that needs it
+    // the buffers themselves are sized by the first run that needs them
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     p->ws_budget = std::min<size_t>(std::max<size_t>(fr / 2, (size_t)64 << 20),
@@ -1400,24 +1459,21 @@ int plan_kernel_stats(libpt_plan *p, double *gemm_ms, int64_t *gemm_launches,
                       double *gemm_flops, double *epi_ms, int64_t *launches) {
   CK(cudaStreamSynchronize(p->st));
   double g = 0.0, e = 0.0, f = 0.0;
-  for (size_t x = 0; x + 1 < p->ev_gemm.size(); x += 2) {
+  ExecTiming &t = p->tm;
+  for (size_t x = 0; x + 1 < t.ev_gemm.size(); x += 2) {
     float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, p->ev_gemm[x], p->ev_gemm[x + 1]));
+    CK(cudaEventElapsedTime(&ms, t.ev_gemm[x], t.ev_gemm[x + 1]));
     g += ms;
-    CK(cudaEventElapsedTime(&ms, p->ev_epi[x], p->ev_epi[x + 1]));
+    CK(cudaEventElapsedTime(&ms, t.ev_epi[x], t.ev_epi[x + 1]));
     e += ms;
   }
-  for (double v : p->flops_gemm) f += v;
+  for (double v : t.flops) f += v;
   if (gemm_ms) *gemm_ms = g;
-  if (gemm_launches) *gemm_launches = (int64_t)(p->ev_gemm.size() / 2);
+  if (gemm_launches) *gemm_launches = (int64_t)(t.ev_gemm.size() / 2);
   if (gemm_flops) *gemm_flops = f;
   if (epi_ms) *epi_ms = e;
   if (launches) *launches = p->launches;
-  for (cudaEvent_t ev : p->ev_gemm) cudaEventDestroy(ev);
-  for (cudaEvent_t ev : p->ev_epi) cudaEventDestroy(ev);
-  p->ev_gemm.clear();
-  p->ev_epi.clear();
-  p->flops_gemm.clear();
+  t.clear();
   p->launches = 0;
   return LIBPT_OK;
 }
@@ -1439,15 +1495,17 @@ size_t rpt_arena_bytes(int64_t o, int64_t v, int64_t nb) {
   const int64_t st_aaa = pad32(v * pad4(np));
   const int64_t st_aab = 2 * pad32(v * v * pad4(v)) + pad32(v * pad4(np));
   const int64_t stride = std::max(st_aaa, st_aab);
+  s += 2 * (r(sizeof(TcMapSet)) + r(sizeof(EpiArgs)));   // views per case
   s += r(nb * stride * 8) + r(nb * ntl * 8) +
-       r(nb * 3 * (int64_t)sizeof(GemmJob)) + r(nb * 12) + r(nb * 4);
+       r((int64_t)Executor::bytes_for((size_t)nb, 3));
   return s;
 }
 
 void plan_destroy(libpt_plan *p) {
   if (!p) return;
-  for (cudaEvent_t ev : p->ev_gemm) cudaEventDestroy(ev);
-  for (cudaEvent_t ev : p->ev_epi) cudaEventDestroy(ev);
+  if (p->st) cudaStreamSynchronize(p->st);
+  p->tm.clear();
+  if (p->exec_ready) p->exec.destroy();
   for (void *a : p->allocs) cudaFree(a);
   delete p;
 }
@@ -1464,19 +1522,16 @@ double plan_flops(const libpt_plan *p, int64_t first, int64_t n) {
 
 int plan_run(libpt_plan *p, const int64_t *idx, size_t n) {
   const int64_t total = (int64_t)p->queue.size();
-  std::vector<std::vector<int64_t>> per(p->cases.size());
+  std::vector<int64_t> ents(n);
   for (size_t x = 0; x < n; ++x) {
     const int64_t q = idx ? idx[x] : (int64_t)x;
     if (q < 0 || q >= total) {
       set_error("libpt_plan_run: queue index out of range");
       return LIBPT_ERR_ARG;
     }
-    per[p->queue[q].x].push_back(q);
+    ents[x] = q;
   }
-  for (size_t ci = 0; ci < p->cases.size(); ++ci)
-    if (!per[ci].empty())
-      if (int r = run_case(p, p->cases[ci], per[ci])) return r;
-  return LIBPT_OK;
+  return run_entries(p, ents);
 }
 
 int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e) {

@@ -5,11 +5,25 @@
 #include <vector>
 
 #include "engine.h"
+#include "exec.h"
+#include "pt.h"
 
 namespace ptb {
 
 void set_error(const std::string &msg);
 const char *last_error();
+
+// Returns a LIBPT_ERR_* status (after recording the message) when a CUDA
+// runtime call fails.
+#define CK(call)                                                          \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess) {                                              \
+      ::ptb::set_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+      return e_ == cudaErrorMemoryAllocation ? LIBPT_ERR_NOMEM            \
+                                             : LIBPT_ERR_CUDA;            \
+    }                                                                     \
+  } while (0)
 // Host allocations through the libpt_set_malloc / libpt_set_free hooks.
 void *host_alloc(size_t n);
 void host_free(void *p);
@@ -79,9 +93,12 @@ struct SpinCase {
   int64_t first = 0, count = 0;         // range in the triples queue
   MapSet maps;
   std::vector<JobT> jobs;               // per-triple job templates
-  EpiArgs epi;                          // fixed part of the epilogue args
+  EpiArgs epi;                          // fixed epilogue arguments
+  EpiArgs *d_epi = nullptr;             // ... in device memory
+  int64_t ws_stride = 0;                // doubles of contraction output
   int4 *d_tiles = nullptr;
   int ntiles = 0, ctiles = 0;
+  CUtensorMap *d_maps = nullptr;        // the kernel's views, device memory
   double flops_per_triple = 0.0;        // reference GEMM flops
   int bm = GEMM_BM;                     // CTA tile rows of this case's GEMMs
   OpDesc opd[MAX_MAPS];                 // operand behind each DMMA map
@@ -106,18 +123,22 @@ struct libpt_plan {
   std::vector<ptb::SpinCase> cases;
   std::vector<int4> queue;              // (case, i, j, k)
   double *e_slot = nullptr;
-  // batch resources
+  // round resources: contraction outputs (packed by each triple's own
+  // size), partial energies and descriptors of one round of triples
   double *ws = nullptr;
-  size_t ws_bytes = 0;                  // current workspace allocation
-  size_t ws_budget = 0;                 // workspace size limit
   double *partials = nullptr;
-  size_t partials_cap = 0;
-  ptb::GemmJob *d_jobs = nullptr;
-  size_t jobs_cap = 0;
-  int *d_trip = nullptr, *d_slot = nullptr;
-  size_t trip_cap = 0;
+  char *d_desc = nullptr;
+  int64_t ws_cap = 0, part_cap = 0;     // doubles held
+  size_t tri_cap = 0;                   // triples a round may hold
+  size_t ws_budget = 0;                 // workspace size limit (bytes)
+  int64_t ws_stride = 0;                // max over cases (doubles)
+  int64_t ws_stride_min = 0;            // min over cases (doubles)
+  int ntiles_max = 0;                   // max epilogue tiles of a triple
+  size_t jobs_max = 0;                  // max GEMM jobs of a triple
   unsigned *d_err = nullptr;
   size_t max_batch = 0;                 // 0: derive from the memory budget
+  ptb::Executor exec;                   // the plan's own rounds
+  bool exec_ready = false;
   // caller-provided device arena: when set, every device buffer of the plan
   // is carved from it and nothing is allocated or freed
   char *arena = nullptr;
@@ -129,10 +150,10 @@ struct libpt_plan {
   ptb::I8Tile i8tile{64, 32};           // emulated FP64 tile variant
   std::vector<std::pair<std::pair<const double *, int>, signed char *>> i8planes;
   std::vector<ptb::Family> fams;
-  // kernel timing (libpt_plan_timing): events around each launch
+  // kernel timing (libpt_plan_timing): events around each round's GEMMs
+  // and epilogues
   bool timing = false;
-  std::vector<cudaEvent_t> ev_gemm, ev_epi;  // start/stop pairs
-  std::vector<double> flops_gemm;            // algorithmic flops per launch
+  ptb::ExecTiming tm;
   int64_t launches = 0;                      // kernels launched by runs
 };
 
@@ -166,6 +187,17 @@ int dmma_map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R,
 int dmma_map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld,
                int64_t K, int64_t P);
 int plan_run(libpt_plan *p, const int64_t *idx, size_t n);
+// Where the next triple of a plan goes in its round resources.
+struct PlanCursor {
+  int64_t ws = 0, part = 0;
+  size_t triples = 0;
+};
+// Appends queue entries ents[0..n) of plan p to a round while they fit the
+// plan's round resources (from cur on); *taken = entries appended.
+int plan_append(libpt_plan *p, const int64_t *ents, size_t n, PlanCursor &cur,
+                Round &r, size_t *taken);
+// The GEMM variant that runs a plan's spin case.
+GemmGroup plan_group(const libpt_plan *p, const SpinCase &c);
 int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e);
 void plan_destroy(libpt_plan *p);
 double plan_flops(const libpt_plan *p, int64_t first, int64_t n);

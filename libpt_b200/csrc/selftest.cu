@@ -75,6 +75,7 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
   using namespace ptb;
   int slices = (precision >> 8) & 0xFF;
   const int variant = (precision >> 16) & 0xFF;
+  const bool dev_maps = ((precision >> 24) & 0xFF) != 0;
   precision &= 0xFF;
   if (slices == 0) slices = 6;
   const I8Tile *tiles = nullptr;
@@ -111,7 +112,9 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
   double *Ca = (double *)alloc((size_t)m * np * 8);
   unsigned *err = (unsigned *)alloc(4);
   GemmJob *dj = (GemmJob *)alloc(sizeof(GemmJob));
-  if (!A || !B1 || !B2 || !Cm || !Cr || !Ca || !err || !dj) {
+  GemmList *dl = (GemmList *)alloc(sizeof(GemmList));
+  CUtensorMap *dmaps = (CUtensorMap *)alloc(sizeof(TcMapSet));
+  if (!A || !B1 || !B2 || !Cm || !Cr || !Ca || !err || !dj || !dl || !dmaps) {
     set_error("libpt_selftest: cudaMalloc failed");
     return done(LIBPT_ERR_NOMEM);
   }
@@ -133,6 +136,27 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
   int r = LIBPT_OK;
   cudaError_t ce = cudaSuccess;
   std::function<cudaError_t()> launch;
+  int grid = 0, nt = 0;
+  // the job, its one-entry work list and its views, in device memory
+  // views as kernel parameters (bits 24-31 of the precision word select
+  // device-memory views instead)
+  LaunchMaps pm_host;
+  const LaunchMaps *pmaps = dev_maps ? nullptr : &pm_host;
+  auto publish = [&](const void *maps, size_t bytes) {
+    job.maps = dmaps;
+    job.map0 = 0;
+    job.tile_begin = 0;
+    std::memcpy(&pm_host, maps, bytes < sizeof(pm_host) ? bytes : sizeof(pm_host));
+    GemmList l;
+    l.jobs = dj;
+    l.njobs = 1;
+    l.ntiles = job.mtiles * job.ntiles_n;
+    nt = l.ntiles;
+    grid = l.ntiles < GEMM_GRID ? l.ntiles : GEMM_GRID;
+    cudaMemcpy(dmaps, maps, bytes, cudaMemcpyHostToDevice);
+    cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
+    cudaMemcpy(dl, &l, sizeof(l), cudaMemcpyHostToDevice);
+  };
   if (precision == LIBPT_PREC_FP64) {
     MapSet maps;
     memset(&maps, 0, sizeof(maps));
@@ -149,11 +173,8 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
       job.seg[s].neg = (int16_t)s;
       job.seg[s].ksteps = (k + GEMM_BK - 1) / GEMM_BK;
     }
-    cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
-    launch = [=]() {
-      return gemm_dmma_launch(maps, dj, 1, job.mtiles * job.ntiles_n, bm, err,
-                              nullptr);
-    };
+    publish(&maps, sizeof(maps));
+    launch = [=]() { return gemm_dmma_launch(dj, dl, 1, nt, pmaps, bm, grid, err, nullptr); };
   } else if (precision == LIBPT_PREC_EMU64) {
     // one A family (A itself) and one B family (B1 part 0, B2 part 1)
     const int S = slices;
@@ -202,10 +223,9 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
       job.seg[s2].neg = (int16_t)s2;
       job.seg[s2].ksteps = (k + kc - 1) / kc;
     }
-    cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
+    publish(&tcmaps_scratch(), sizeof(TcMapSet));
     launch = [=]() {
-      return gemm_i8_launch(S, tl, tcmaps_scratch(), dj, 1,
-                            job.mtiles * job.ntiles_n, err, nullptr);
+      return gemm_i8_launch(S, tl, dj, dl, 1, nt, pmaps, grid, err, nullptr);
     };
   } else {
     float *pl[6];
@@ -248,11 +268,8 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
       pr.pb[q] = pb[q];
     }
     pr.n = 3;
-    cudaMemcpy(dj, &job, sizeof(job), cudaMemcpyHostToDevice);
-    launch = [=]() {
-      return gemm_tc_launch(TC_TF32, maps, dj, 1, job.mtiles * job.ntiles_n,
-                            pr, err, nullptr);
-    };
+    publish(&maps, sizeof(maps));
+    launch = [=]() { return gemm_tc_launch(dj, dl, 1, nt, pmaps, grid, pr, err, nullptr); };
   }
   if (ce == cudaSuccess) ce = launch();
   if (ce == cudaSuccess) ce = cudaDeviceSynchronize();

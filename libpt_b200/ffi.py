@@ -133,21 +133,23 @@ def solve_device(case, tensors, mp=False, stream=None):
     return e.value
 
 
-def selftest(precision, m, n, k, variant=0):
-    """Error of one contraction kernel (tile variant `variant`) against an
-    FP64 product, over the dot products' magnitude scale (libpt_selftest)."""
+def selftest(precision, m, n, k, variant=0, device_maps=False):
+    """Error of one contraction kernel (tile variant `variant`; tensor maps
+    from device memory when device_maps) against an FP64 product, over the
+    dot products' magnitude scale (libpt_selftest)."""
     e = ctypes.c_double(-1.0)
-    check(lib().libpt_selftest(precision | (variant << 16), m, n, k,
-                               ctypes.byref(e)))
+    word = precision | (variant << 16) | ((1 << 24) if device_maps else 0)
+    check(lib().libpt_selftest(word, m, n, k, ctypes.byref(e)))
     return e.value
 
 
-def kernel_bench(precision, m, n, k, reps=10, variant=0):
+def kernel_bench(precision, m, n, k, reps=10, variant=0, device_maps=False):
     """(mean ms per launch, check error) of one resident contraction job of
     4 m n k flops (libpt_kernel_bench)."""
     ms, e = ctypes.c_double(0.0), ctypes.c_double(-1.0)
-    check(lib().libpt_kernel_bench(precision | (variant << 16), m, n, k, reps,
-                                   ctypes.byref(ms), ctypes.byref(e)))
+    word = precision | (variant << 16) | ((1 << 24) if device_maps else 0)
+    check(lib().libpt_kernel_bench(word, m, n, k, reps, ctypes.byref(ms),
+                                   ctypes.byref(e)))
     return ms.value, e.value
 
 

@@ -43,3 +43,14 @@ def test_tcgen05_int8_emulated_fp64(slices, variant, m, n, k):
     prec = ffi.PREC_EMU64 | (slices << 8)
     assert ffi.selftest_variants(prec) == I8_VARIANTS[slices]
     assert ffi.selftest(prec, m, n, k, variant) < EMU_BOUND[slices]
+
+
+@pytest.mark.parametrize("m,n,k", [(5, 7, 3), (300, 520, 700)])
+def test_device_memory_tensor_maps(m, n, k):
+    """The form batched multi-solve launches use: tensor maps read from
+    device memory (fenced per CTA) instead of kernel parameters."""
+    assert ffi.selftest(ffi.PREC_FP64, m, n, k, 0, device_maps=True) < 1e-14
+    assert ffi.selftest(ffi.PREC_TF32X3, m, n, k, device_maps=True) < 5e-5
+    for s in (4, 6):
+        prec = ffi.PREC_EMU64 | (s << 8)
+        assert ffi.selftest(prec, m, n, k, 0, device_maps=True) < EMU_BOUND[s]
