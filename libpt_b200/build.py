@@ -26,7 +26,7 @@ HOST_CXX = "/usr/bin/g++"   # the image's $CXX wrapper lacks some runtime specs
 
 SOURCES = ["gemm_dmma.cu", "gemm_tc.cu", "gemm_i8.cu", "epilogue.cu", "prep.cu",
            "exec.cu", "plan.cu", "tune.cpp", "api.cpp", "noalloc.cu",
-           "selftest.cu"]
+           "selftest.cu", "server.cpp"]
 HEADERS = ["common.cuh", "engine.h", "exec.h", "plan.h", "tune.h"]
 
 

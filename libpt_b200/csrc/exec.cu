@@ -220,7 +220,7 @@ int Executor::launch_all(const std::vector<GemmGroup> &groups,
 }
 
 int Executor::run(Round &r, unsigned *d_err, ExecTiming *timing,
-                  int64_t *launches) {
+                  int64_t *launches, bool replay) {
   if (r.empty()) return LIBPT_OK;
   std::vector<GemmGroup> groups;
   for (auto &kv : r.gemm)
@@ -317,7 +317,7 @@ int Executor::run(Round &r, unsigned *d_err, ExecTiming *timing,
     CK(cudaEventRecord(copied_[parity_], st_));
     parity_ ^= 1;
   }
-  if (!graphs_ || timing)
+  if (!graphs_ || timing || !replay)
     return launch_all(groups, d_err, epi_on, timing, &r, launches);
   // graph replay keyed by the variant set
   std::string key;
@@ -350,6 +350,7 @@ int Executor::run(Round &r, unsigned *d_err, ExecTiming *timing,
     return LIBPT_OK;
   }
   CK(cudaGraphLaunch(it->second, st_));
+  ++replays_;
   if (launches) {
     *launches += (int64_t)groups.size() + 1;
     for (int a = 0; a < 2; ++a)

@@ -76,7 +76,11 @@ class Executor {
                           bool graphs = false);
   // Launches the round on the stream (asynchronous).  d_err: device error
   // word the kernels set on a timed-out wait.  Returns the kernels launched.
-  int run(Round &r, unsigned *d_err, ExecTiming *timing, int64_t *launches);
+  // replay: use (or capture) the CUDA graph of the round's variant set
+  // (graph-capable executors only); otherwise launch directly.
+  int run(Round &r, unsigned *d_err, ExecTiming *timing, int64_t *launches,
+          bool replay = true);
+  int64_t graph_replays() const { return replays_; }
   cudaStream_t stream() const { return st_; }
 
  private:
@@ -94,6 +98,7 @@ class Executor {
   std::map<std::string, cudaGraphExec_t> cache_;
   LaunchMaps pmaps_;   // staging of a launch's parameter-table maps
   size_t slot_jobs_ = 0;                 // graphs: jobs per GEMM slot
+  int64_t replays_ = 0;
   std::vector<const GemmJob *> gjobs_;   // device job arrays of the groups
   int epi_grid_[2][2] = {{0, 0}, {0, 0}};
 };

@@ -77,8 +77,15 @@ LIBPT_API int libpt_rpt_dev_static(size_t oa, size_t va, const double *d_ov,
     ptb::set_error("e_out is NULL");
     return LIBPT_ERR_ARG;
   }
-  // size check first, from the sizes alone (one triple per batch at least)
-  const size_t need = ptb::rpt_arena_bytes((int64_t)oa, (int64_t)va, 1);
+  // size check first, from the sizes alone: a cheap lower bound (the padded
+  // amplitude and OVVV copies), then the exact footprint of a plan whose
+  // rounds hold one triple at least (sizing pass, no device work)
+  const double lower = 8.0 * ((double)oa * oa * va * va * 2 +
+                              (double)oa * va * va * va);
+  const size_t need =
+      (oa > 4096 || va > 4096 || lower > (double)LIBPT_STATIC_SCRATCH_BYTES)
+          ? (size_t)lower
+          : ptb::plan_footprint(0, oa, va, oa, va, 0, LIBPT_PREC_FP64, false, 1);
   if (oa > 4096 || va > 4096 || need > (size_t)LIBPT_STATIC_SCRATCH_BYTES) {
     ptb::set_error("libpt_rpt_dev_static: o=" + std::to_string(oa) +
                    ", v=" + std::to_string(va) + " needs " +

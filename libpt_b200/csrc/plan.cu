@@ -27,6 +27,17 @@ namespace ptb {
 
 static thread_local std::string g_last_error;
 void set_error(const std::string &msg) { g_last_error = msg; }
+
+// Sizing pass (plan_footprint): plan creation runs its host logic with
+// device allocations carved from a fake arena and every device operation
+// skipped, so the arena's high-water mark is the plan's exact footprint.
+static thread_local bool g_dry = false;
+
+// A device operation of plan creation: skipped in the sizing pass.
+#define DEV(call)                                                          \
+  do {                                                                     \
+    if (!g_dry) CK(call);                                                  \
+  } while (0)
 const char *last_error() { return g_last_error.c_str(); }
 
 namespace {
@@ -61,6 +72,7 @@ EncodeTiledFn encode_fn() {
 // box (4, bm, 1, 1).
 int map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R, int64_t Q,
           int64_t P, int bm) {
+  if (g_dry) return LIBPT_OK;   // sizing pass: no views needed
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -90,6 +102,7 @@ int map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R, int64_t Q,
 // box (4, GEMM_BK, 1).
 int map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld, int64_t K,
           int64_t P) {
+  if (g_dry) return LIBPT_OK;   // sizing pass: no views needed
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -114,6 +127,7 @@ int map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld, int64_t K,
 
 int tc_encode(CUtensorMap *m, const float *p, int rank, const cuuint64_t *dims,
               const cuuint64_t *strides, const cuuint32_t *box) {
+  if (g_dry) return LIBPT_OK;   // sizing pass: no views needed
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -141,6 +155,7 @@ int dalloc(libpt_plan *p, void **ptr, size_t bytes);
 // to 32 bytes.  A: (32, R, nK, Q*P, 2S); B: (32, N, nK, P, S).
 int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
              int64_t Q, int64_t P, int S) {
+  if (g_dry) return LIBPT_OK;   // sizing pass: no views needed
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -167,6 +182,7 @@ int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
 
 int i8_map_b(CUtensorMap *m, const signed char *p, int64_t K, int64_t N,
              int64_t P, int S, int bn) {
+  if (g_dry) return LIBPT_OK;   // sizing pass: no views needed
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled unavailable");
@@ -242,12 +258,12 @@ int get_planes(libpt_plan *p, const OpDesc &d, Planes *out) {
     const int64_t n = d.P * d.Q * d.R * kp;
     if (dalloc(p, (void **)&pl.hi, n * 4) || dalloc(p, (void **)&pl.lo, n * 4))
       return LIBPT_ERR_NOMEM;
-    CK(split_tf32_launch(d.src, pl.hi, pl.lo, n, p->st));
+    DEV(split_tf32_launch(d.src, pl.hi, pl.lo, n, p->st));
   } else {
     const int64_t n = d.P * d.N * kp;
     if (dalloc(p, (void **)&pl.hi, n * 4) || dalloc(p, (void **)&pl.lo, n * 4))
       return LIBPT_ERR_NOMEM;
-    CK(transpose_split_tf32_launch(d.src, pl.hi, pl.lo, d.P, (int)d.K, d.N,
+    DEV(transpose_split_tf32_launch(d.src, pl.hi, pl.lo, d.P, (int)d.K, d.N,
                                    d.Nld, kp, p->st));
   }
   p->planes.push_back({key, pl});
@@ -307,6 +323,7 @@ int dalloc(libpt_plan *p, void **ptr, size_t bytes) {
 struct Uploader {
   libpt_plan *p;
   bool host, fp32;
+  size_t stage_cap = (size_t)256 << 20;   // staging buffer bound
   void *stage = nullptr;
   size_t stage_bytes = 0;
 
@@ -316,23 +333,23 @@ struct Uploader {
     const size_t es = fp32 ? 4 : 8;
     if (!host) {
       if (w == dpitch && !fp32)
-        CK(cudaMemcpyAsync(dst, src, (size_t)rows * w * 8,
+        DEV(cudaMemcpyAsync(dst, src, (size_t)rows * w * 8,
                            cudaMemcpyDeviceToDevice, p->st));
       else
-        CK(repack_launch(src, fp32, dst, rows, w, dpitch, p->st));
+        DEV(repack_launch(src, fp32, dst, rows, w, dpitch, p->st));
       return LIBPT_OK;
     }
     if (!stage) {
-      stage_bytes = (size_t)256 << 20;
+      stage_bytes = stage_cap;
       if (dalloc(p, &stage, stage_bytes)) return LIBPT_ERR_NOMEM;
     }
     if (w == dpitch) {   // unpadded: copy as a flat array
       const int64_t total = rows * w, chunk = (int64_t)(stage_bytes / es);
       for (int64_t x0 = 0; x0 < total; x0 += chunk) {
         const int64_t nx = std::min(chunk, total - x0);
-        CK(cudaMemcpyAsync(stage, (const char *)src + (size_t)x0 * es,
+        DEV(cudaMemcpyAsync(stage, (const char *)src + (size_t)x0 * es,
                            (size_t)nx * es, cudaMemcpyHostToDevice, p->st));
-        CK(repack_launch(stage, fp32, dst + x0, 1, nx, nx, p->st));
+        DEV(repack_launch(stage, fp32, dst + x0, 1, nx, nx, p->st));
       }
       return LIBPT_OK;
     }
@@ -340,9 +357,9 @@ struct Uploader {
         std::max<int64_t>(1, (int64_t)(stage_bytes / (es * std::max<int64_t>(w, 1))));
     for (int64_t r0 = 0; r0 < rows; r0 += chunk) {
       const int64_t nr = std::min(chunk, rows - r0);
-      CK(cudaMemcpyAsync(stage, (const char *)src + (size_t)r0 * w * es,
+      DEV(cudaMemcpyAsync(stage, (const char *)src + (size_t)r0 * w * es,
                          (size_t)nr * w * es, cudaMemcpyHostToDevice, p->st));
-      CK(repack_launch(stage, fp32, dst + r0 * dpitch, nr, w, dpitch, p->st));
+      DEV(repack_launch(stage, fp32, dst + r0 * dpitch, nr, w, dpitch, p->st));
     }
     return LIBPT_OK;
   }
@@ -423,7 +440,7 @@ int upload_set(libpt_plan *p, Uploader &up, const Sizes &S, OperandSet &set,
     const int64_t o = s ? S.ob : S.oa, v = s ? S.vb : S.va;
     const int64_t ldp = pad4(npair(v));
     if (dalloc(p, (void **)&set.taup[s], o * o * ldp * 8)) return LIBPT_ERR_NOMEM;
-    CK(pack_pairs_launch(set.tau[s ? 2 : 0], set.taup[s], o * o, (int)v,
+    DEV(pack_pairs_launch(set.tau[s ? 2 : 0], set.taup[s], o * o, (int)v,
                          pad4(v), ldp, p->st));
   }
   return LIBPT_OK;
@@ -592,9 +609,9 @@ int build_aaa(libpt_plan *p, SpinCase &c) {
   c.ctiles = 1;
   if (c.ntiles) {
     if (dalloc(p, (void **)&c.d_tiles, tiles.size() * sizeof(int4))) return LIBPT_ERR_NOMEM;
-    CK(cudaMemcpyAsync(c.d_tiles, tiles.data(), tiles.size() * sizeof(int4),
+    DEV(cudaMemcpyAsync(c.d_tiles, tiles.data(), tiles.size() * sizeof(int4),
                        cudaMemcpyHostToDevice, p->st));
-    CK(cudaStreamSynchronize(p->st));
+    DEV(cudaStreamSynchronize(p->st));
   }
   e.ntiles = c.ntiles;
   e.tiles = c.d_tiles;
@@ -721,9 +738,9 @@ int build_aab(libpt_plan *p, SpinCase &c) {
   c.ntiles = (int)tiles.size() * c.ctiles;
   if (!tiles.empty()) {
     if (dalloc(p, (void **)&c.d_tiles, tiles.size() * sizeof(int4))) return LIBPT_ERR_NOMEM;
-    CK(cudaMemcpyAsync(c.d_tiles, tiles.data(), tiles.size() * sizeof(int4),
+    DEV(cudaMemcpyAsync(c.d_tiles, tiles.data(), tiles.size() * sizeof(int4),
                        cudaMemcpyHostToDevice, p->st));
-    CK(cudaStreamSynchronize(p->st));
+    DEV(cudaStreamSynchronize(p->st));
   }
   e.ntiles = c.ntiles;
   e.tiles = c.d_tiles;
@@ -745,8 +762,10 @@ Family *family(libpt_plan *p, int id, int64_t n) {
   if (dalloc(p, (void **)&f.max0, n * 8 + 8) ||
       dalloc(p, (void **)&f.max1, n * 8 + 8) || dalloc(p, (void **)&f.e, n + 16))
     return nullptr;
-  cudaMemsetAsync(f.max0, 0, n * 8 + 8, p->st);
-  cudaMemsetAsync(f.max1, 0, n * 8 + 8, p->st);
+  if (!g_dry) {
+    cudaMemsetAsync(f.max0, 0, n * 8 + 8, p->st);
+    cudaMemsetAsync(f.max1, 0, n * 8 + 8, p->st);
+  }
   p->fams.push_back(f);
   return &p->fams.back();
 }
@@ -767,9 +786,9 @@ int i8_maxima(libpt_plan *p) {
       seen.push_back(key);
       unsigned long long *m = d.part ? f->max1 : f->max0;
       if (d.role == 0)
-        CK(rowmax_launch(d.src, d.P * d.Q, d.R, d.K, pad4(d.K), m, p->st));
+        DEV(rowmax_launch(d.src, d.P * d.Q, d.R, d.K, pad4(d.K), m, p->st));
       else
-        CK(colmax_launch(d.src, d.P, d.K, d.N, d.w, d.wsrc, d.ldsrc, m, p->st));
+        DEV(colmax_launch(d.src, d.P, d.K, d.N, d.w, d.wsrc, d.ldsrc, m, p->st));
     }
   }
   return LIBPT_OK;
@@ -786,9 +805,9 @@ int i8_exponents(libpt_plan *p) {
       if (f.id >= 100 || f.id / 8 != x) continue;   // A families of set x
       for (int part = 0; part < 2; ++part) {
         h.assign(f.n, 0);
-        CK(cudaMemcpyAsync(h.data(), part ? f.max1 : f.max0, f.n * 8,
-                           cudaMemcpyDeviceToHost, p->st));
-        CK(cudaStreamSynchronize(p->st));
+        DEV(cudaMemcpyAsync(h.data(), part ? f.max1 : f.max0, f.n * 8,
+                            cudaMemcpyDeviceToHost, p->st));
+        DEV(cudaStreamSynchronize(p->st));
         for (unsigned long long u : h) {
           double v;
           memcpy(&v, &u, 8);
@@ -803,7 +822,7 @@ int i8_exponents(libpt_plan *p) {
     const int set = (f.id % 100) / 8;
     const int k = (set ? p->R : p->L).balance;
     const double s1 = std::ldexp(1.0, f.id >= 100 ? k : -k);
-    CK(exps_launch(f.max0, f.max1, s1, f.n, f.e, p->st));
+    DEV(exps_launch(f.max0, f.max1, s1, f.n, f.e, p->st));
   }
   return LIBPT_OK;
 }
@@ -843,13 +862,13 @@ int i8_planes(libpt_plan *p, SpinCase &c) {
       if (d.role == 0) {
         const int64_t n = d.P * d.Q * d.R * kpi;
         if (dalloc(p, (void **)&pl, 2 * S * n)) return LIBPT_ERR_NOMEM;
-        CK(slice_a_launch(d.src, d.P * d.Q, d.R, d.K, pad4(d.K), kpi,
+        DEV(slice_a_launch(d.src, d.P * d.Q, d.R, d.K, pad4(d.K), kpi,
                           std::ldexp(1.0, d.part ? -k : 0), f->e, S, pl,
                           p->st));
       } else {
         const int64_t n = d.P * d.N * kpi;
         if (dalloc(p, (void **)&pl, S * n)) return LIBPT_ERR_NOMEM;
-        CK(slice_b_launch(d.src, d.P, (int)d.K, d.N, d.w, d.wsrc, d.ldsrc, kpi,
+        DEV(slice_b_launch(d.src, d.P, (int)d.K, d.N, d.w, d.wsrc, d.ldsrc, kpi,
                           std::ldexp(1.0, d.part ? k : 0), f->e, S, pl,
                           p->st));
       }
@@ -939,12 +958,12 @@ int upload_views(libpt_plan *p) {
                           : (const void *)&c.tcmaps;
     const size_t n = p->precision == LIBPT_PREC_FP64 ? sizeof(MapSet)
                                                      : sizeof(TcMapSet);
-    CK(cudaMemcpyAsync(c.d_maps, src, n, cudaMemcpyHostToDevice, p->st));
-    CK(cudaMemcpyAsync(c.d_epi, &c.epi, sizeof(EpiArgs),
+    DEV(cudaMemcpyAsync(c.d_maps, src, n, cudaMemcpyHostToDevice, p->st));
+    DEV(cudaMemcpyAsync(c.d_epi, &c.epi, sizeof(EpiArgs),
                        cudaMemcpyHostToDevice, p->st));
   }
   // the sources are members of the plan, copied before they can change
-  CK(cudaStreamSynchronize(p->st));
+  DEV(cudaStreamSynchronize(p->st));
   return LIBPT_OK;
 }
 
@@ -1268,7 +1287,7 @@ int autotune(libpt_plan *p) {
 int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
                 const void *const *args, int dtype, int precision, bool host,
                 cudaStream_t st, libpt_plan **out, void *arena,
-                size_t arena_size) {
+                size_t arena_size, size_t arena_nb) {
   *out = nullptr;
   if (kind < 0 || kind > 3 || dtype < 0 || dtype > 1 || !args) {
     set_error("libpt_plan_create: bad kind/dtype/args");
@@ -1284,10 +1303,6 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
   if (slices == 0) slices = 6;
   if (slices < TC_S_MIN || slices > TC_S_MAX) {
     set_error("libpt_plan_create: emulated FP64 takes 4 to 7 slices");
-    return LIBPT_ERR_ARG;
-  }
-  if (arena && precision != LIBPT_PREC_FP64) {
-    set_error("libpt_plan_create: the static scratch serves the FP64 path");
     return LIBPT_ERR_ARG;
   }
   const bool unr = kind == 1 || kind == 3, ft = kind >= 2;
@@ -1329,6 +1344,19 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
   do {
     Sizes S{(int64_t)oa, (int64_t)va, (int64_t)ob, (int64_t)vb};
     Uploader up{p, host, dtype == 1};
+    {
+      // staging: no larger than the largest argument array (256 MiB at most)
+      int64_t big = (int64_t)(oa * va + (unr ? ob * vb : 0));
+      int64_t t2 = 0, oo = 0, vv = 0;
+      for (int b = 0; b < (unr ? 4 : 2); ++b) {
+        t2 += S.oovv(b);
+        oo += S.oovo(b);
+        vv += S.ovvv(b);
+      }
+      big = std::max({big, t2, oo, vv});
+      const size_t bytes = (size_t)big * (dtype ? 4 : 8);
+      up.stage_cap = std::max<size_t>(256, std::min(up.stage_cap, (bytes + 255) & ~size_t(255)));
+    }
     const int64_t nov = (int64_t)(oa * va + (unr ? ob * vb : 0));
     if ((r = dalloc(p, (void **)&p->d_ov, nov * 8 + 8))) break;
     if ((r = dalloc(p, (void **)&p->ov1, nov * 8 + 8))) break;
@@ -1358,7 +1386,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       if (!r) r = upload_set(p, up, S, p->R, args[3], args[6], args[7]);  // t2, i2, i3
     }
     if (r) break;
-    if (cudaStreamSynchronize(st) != cudaSuccess) {
+    if (!g_dry && cudaStreamSynchronize(st) != cudaSuccess) {
       set_error(std::string("preparing operands: ") +
                 cudaGetErrorString(cudaGetLastError()));
       r = LIBPT_ERR_CUDA;
@@ -1368,7 +1396,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     if (p->precision != LIBPT_PREC_FP64) {
       // the tensor-core paths read planes; of the padded FP64 blocks only the
       // amplitudes stay (the energy epilogue's disconnected term reads them)
-      if (cudaStreamSynchronize(st) != cudaSuccess) {
+      if (!g_dry && cudaStreamSynchronize(st) != cudaSuccess) {
         set_error("preparing tensor-core planes failed");
         r = LIBPT_ERR_CUDA;
         break;
@@ -1387,12 +1415,13 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
         }
     }
     if ((r = dalloc(p, (void **)&p->e_slot, (p->queue.size() + 1) * 8))) break;
-    if (cudaMemsetAsync(p->e_slot, 0, (p->queue.size() + 1) * 8, st) != cudaSuccess) {
+    if (!g_dry &&
+        cudaMemsetAsync(p->e_slot, 0, (p->queue.size() + 1) * 8, st) != cudaSuccess) {
       r = LIBPT_ERR_CUDA;
       break;
     }
     if ((r = dalloc(p, (void **)&p->d_err, sizeof(unsigned)))) break;
-    if (cudaMemsetAsync(p->d_err, 0, sizeof(unsigned), st) != cudaSuccess) {
+    if (!g_dry && cudaMemsetAsync(p->d_err, 0, sizeof(unsigned), st) != cudaSuccess) {
       r = LIBPT_ERR_CUDA;
       break;
     }
@@ -1418,8 +1447,9 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       const size_t slack = 3 * 256 + d0;
       const size_t left =
           p->arena_size > used + slack ? p->arena_size - used - slack : 0;
-      const size_t nb = std::min<size_t>({left / per, (size_t)4096,
-                                          p->queue.size()});
+      size_t nb = std::min<size_t>({left / per, (size_t)4096,
+                                    p->queue.size()});
+      if (arena_nb) nb = std::min(nb, arena_nb);
       if (nb == 0) {
         set_error("scratch arena too small for one triple");
         r = LIBPT_ERR_NOMEM;
@@ -1446,7 +1476,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     p->ws_budget = std::min<size_t>(std::max<size_t>(fr / 2, (size_t)64 << 20),
                                     (size_t)16 << 30);
   } while (0);
-  if (!r) r = autotune(p);
+  if (!r && !g_dry) r = autotune(p);
   if (r) {
     plan_destroy(p);
     return r;
@@ -1478,27 +1508,22 @@ int plan_kernel_stats(libpt_plan *p, double *gemm_ms, int64_t *gemm_launches,
   return LIBPT_OK;
 }
 
-size_t rpt_arena_bytes(int64_t o, int64_t v, int64_t nb) {
-  auto r = [](int64_t b) {
-    return (size_t)((std::max<int64_t>(b, 1) + 255) & ~int64_t(255));
-  };
-  const int64_t np = npair(v);
-  size_t s = 3 * r(o * v * 8 + 8) + 2 * r(o * o * v * v * 8 + 8);
-  s += 2 * r(o * o * v * pad4(v) * 8) + 2 * r(o * o * v * pad4(o) * 8) +
-       r(o * v * pad4(np) * 8) + r(o * v * v * pad4(v) * 8) +
-       r(o * o * pad4(np) * 8);
-  const int64_t nbk = (v + EPI_A - 1) / EPI_A, ncb = (v + EPI_C - 1) / EPI_C;
-  const int64_t ntl = nbk * nbk * ncb;        // bound on tiles of a case
-  s += r(ntl * 16) + r(nbk * nbk * 16);       // tile tables
-  const int64_t nq = o * (o - 1) * (o - 2) / 6 + o * (o - 1) / 2 * o;
-  s += r((nq + 1) * 8) + r(4);
-  const int64_t st_aaa = pad32(v * pad4(np));
-  const int64_t st_aab = 2 * pad32(v * v * pad4(v)) + pad32(v * pad4(np));
-  const int64_t stride = std::max(st_aaa, st_aab);
-  s += 2 * (r(sizeof(TcMapSet)) + r(sizeof(EpiArgs)));   // views per case
-  s += r(nb * stride * 8) + r(nb * ntl * 8) +
-       r((int64_t)Executor::bytes_for((size_t)nb, 3));
-  return s;
+size_t plan_footprint(int kind, size_t oa, size_t va, size_t ob, size_t vb,
+                      int dtype, int precision, bool host, size_t nb) {
+  // a sizing pass over a fake, 256-byte aligned arena of unbounded size
+  static const double dummy = 0.0;
+  const void *args[10];
+  for (int a = 0; a < 10; ++a) args[a] = &dummy;
+  char *const fake = reinterpret_cast<char *>((uintptr_t)1 << 44);
+  libpt_plan *p = nullptr;
+  g_dry = true;
+  const int r = plan_create(kind, oa, va, ob, vb, args, dtype, precision, host,
+                            nullptr, &p, fake, (size_t)1 << 60, nb);
+  g_dry = false;
+  if (r || !p) return 0;
+  const size_t used = p->arena_used;
+  plan_destroy(p);
+  return ((used + 255) & ~size_t(255)) + 256;   // + alignment of the base
 }
 
 void plan_destroy(libpt_plan *p) {
@@ -1534,8 +1559,10 @@ int plan_run(libpt_plan *p, const int64_t *idx, size_t n) {
   return run_entries(p, ents);
 }
 
-int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e) {
+int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e,
+                cudaStream_t rs) {
   const size_t total = p->queue.size();
+  const cudaStream_t st = rs ? rs : p->st;
   // the energy readback buffer comes from the caller's allocation hook
   double *slots = static_cast<double *>(host_alloc((total + 1) * 8));
   if (!slots) {
@@ -1547,11 +1574,11 @@ int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e) {
     ~Guard() { host_free(q); }
   } guard{slots};
   CK(cudaMemcpyAsync(slots, p->e_slot, (total + 1) * 8,
-                     cudaMemcpyDeviceToHost, p->st));
+                     cudaMemcpyDeviceToHost, st));
   unsigned err = 0;
   CK(cudaMemcpyAsync(&err, p->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                     p->st));
-  CK(cudaStreamSynchronize(p->st));
+                     st));
+  CK(cudaStreamSynchronize(st));
   if (err) {
     set_error("a device-side wait exceeded its time limit");
     return LIBPT_ERR_TIMEOUT;

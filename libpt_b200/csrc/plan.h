@@ -161,13 +161,17 @@ namespace ptb {
 
 // args: pt.h tensors of `kind` in the reference's order; `host` selects host
 // (true) or device (false) pointers; dtype 0 = FP64, 1 = FP32.
+// arena: carve every device buffer from [arena, arena + arena_size) (no
+// allocation); arena_nb caps the triples of one round (0: what fits).
 int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
                 const void *const *args, int dtype, int precision, bool host,
                 cudaStream_t st, libpt_plan **out, void *arena = nullptr,
-                size_t arena_size = 0);
-// Device bytes a restricted (T) plan of (o, v) takes from an arena when its
-// batches hold up to nb triples (arena mode, device sources).
-size_t rpt_arena_bytes(int64_t o, int64_t v, int64_t nb);
+                size_t arena_size = 0, size_t arena_nb = 0);
+// Exact device bytes plan_create takes from an arena for these arguments
+// with rounds of up to nb triples (a sizing pass: host logic only, no
+// device work); 0 if the arguments are invalid.
+size_t plan_footprint(int kind, size_t oa, size_t va, size_t ob, size_t vb,
+                      int dtype, int precision, bool host, size_t nb);
 // Tensor-core views of TF32 planes (see engine.h): A planes [P][Q][R][Kp],
 // B planes [P][N][Kp] (Kp = pad4(K) floats per row).
 int tc_map_a(CUtensorMap *m, const float *p, int64_t K, int64_t R, int64_t Q,
@@ -198,7 +202,10 @@ int plan_append(libpt_plan *p, const int64_t *ents, size_t n, PlanCursor &cur,
                 Round &r, size_t *taken);
 // The GEMM variant that runs a plan's spin case.
 GemmGroup plan_group(const libpt_plan *p, const SpinCase &c);
-int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e);
+// Reads the per-triple energies back on stream rs (null: the plan's) and
+// sums them in queue order (restricted factor applied).
+int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e,
+                cudaStream_t rs = nullptr);
 void plan_destroy(libpt_plan *p);
 double plan_flops(const libpt_plan *p, int64_t first, int64_t n);
 int plan_kernel_stats(libpt_plan *p, double *gemm_ms, int64_t *gemm_launches,

@@ -18,6 +18,8 @@ KINDS = ("rpt", "upt", "rft", "uft")
 KIND_ID = {k: i for i, k in enumerate(KINDS)}
 
 LIBPT_OK = 0
+LIBPT_ERR_NOMEM = 2
+LIBPT_ERR_TIMEOUT = 4
 ERRORS = {1: "LIBPT_ERR_ARG", 2: "LIBPT_ERR_NOMEM", 3: "LIBPT_ERR_CUDA",
           4: "LIBPT_ERR_TIMEOUT", 5: "LIBPT_ERR_UNSUPPORTED"}
 PREC_FP64 = 0
@@ -91,6 +93,21 @@ def lib():
     L.libpt_selftest_variants.argtypes = [ctypes.c_int]
     L.libpt_kernel_bench.restype = ctypes.c_int
     L.libpt_kernel_bench.argtypes = [ctypes.c_int] * 5 + [dp, dp]
+    # serving (pt_serve.h)
+    L.libpt_footprint.restype = sz
+    L.libpt_footprint.argtypes = [ctypes.c_int] + [sz] * 4 + [ctypes.c_int] * 3 + [sz]
+    L.libpt_server_create.restype = ctypes.c_int
+    L.libpt_server_create.argtypes = [sz, ctypes.c_int, ctypes.POINTER(vp)]
+    L.libpt_server_submit.restype = ctypes.c_int
+    L.libpt_server_submit.argtypes = ([vp, ctypes.c_int] + [sz] * 4 +
+                                      [ctypes.POINTER(vp)] + [ctypes.c_int] * 3 +
+                                      [ctypes.POINTER(ctypes.c_uint64)])
+    L.libpt_server_wait.restype = ctypes.c_int
+    L.libpt_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, dp, dp]
+    L.libpt_server_stats_get.restype = ctypes.c_int
+    L.libpt_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    L.libpt_server_destroy.restype = ctypes.c_int
+    L.libpt_server_destroy.argtypes = [vp]
     L.libpt_plan_destroy.restype = ctypes.c_int
     L.libpt_plan_destroy.argtypes = [vp]
     _lib = L
@@ -156,6 +173,90 @@ def kernel_bench(precision, m, n, k, reps=10, variant=0, device_maps=False):
 def selftest_variants(precision):
     """Number of tile variants of a precision mode (libpt_selftest_variants)."""
     return lib().libpt_selftest_variants(precision)
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("rounds", ctypes.c_uint64),
+                ("graph_rounds", ctypes.c_uint64), ("triples", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("flops", ctypes.c_double),
+                ("pool_bytes", ctypes.c_size_t),
+                ("bytes_in_use", ctypes.c_size_t),
+                ("peak_bytes_in_use", ctypes.c_size_t),
+                ("max_resident", ctypes.c_uint64)]
+
+
+def footprint(kind, sizes, mp=False, precision=PREC_FP64, host=True,
+              round_triples=0):
+    """Device bytes the server takes for a solve (libpt_footprint)."""
+    s = list(sizes)
+    if len(s) == 2:
+        s += s
+    return lib().libpt_footprint(KIND_ID[kind], *s, 1 if mp else 0, precision,
+                                 1 if host else 0, round_triples)
+
+
+class Server:
+    """Continuous-batching request loop (libpt_server_*, pt_serve.h)."""
+
+    def __init__(self, mem_budget=0, max_active=0):
+        h = ctypes.c_void_p()
+        check(lib().libpt_server_create(mem_budget, max_active,
+                                        ctypes.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, case, tensors=None, mp=False, precision=PREC_FP64):
+        """Queues a solve; tensors: device tensors by name, else the case's
+        host arrays.  Returns its ticket."""
+        kind = case["kind"]
+        s = _sizes(case)
+        if len(s) == 2:
+            s += s
+        names = args_of(kind)
+        if tensors is None:
+            dt = np.float32 if mp else np.float64
+            arrs = [np.ascontiguousarray(case[n], dtype=dt) for n in names]
+            ptrs = (ctypes.c_void_p * len(names))(
+                *[a.ctypes.data for a in arrs])
+            keep, host = arrs, 1
+        else:
+            keep = [tensors[n] for n in names]
+            ptrs = (ctypes.c_void_p * len(names))(*[t.data_ptr() for t in keep])
+            host = 0
+        t = ctypes.c_uint64()
+        check(lib().libpt_server_submit(self.h, KIND_ID[kind], *s, ptrs,
+                                        1 if mp else 0, precision, host,
+                                        ctypes.byref(t)))
+        self._keep[t.value] = keep     # inputs live until the solve is done
+        return t.value
+
+    def wait(self, ticket, timeout=-1.0):
+        """(energy, latency seconds) of a solve."""
+        e, lat = ctypes.c_double(), ctypes.c_double()
+        code = lib().libpt_server_wait(self.h, ticket, timeout,
+                                       ctypes.byref(e), ctypes.byref(lat))
+        if code != LIBPT_ERR_TIMEOUT:   # done: its inputs may go
+            self._keep.pop(ticket, None)
+        check(code)
+        return e.value, lat.value
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().libpt_server_stats_get(self.h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib().libpt_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Plan:
