@@ -978,15 +978,16 @@ int ensure_capacity(libpt_plan *p, const std::vector<int64_t> &ents) {
     biggest = std::max(biggest, st);
     if (want * 8 >= (int64_t)p->ws_budget) break;
   }
+  if (p->arena) {   // fixed resources: rounds are cut to what they hold
+    if (p->tri_cap >= 1 && biggest <= p->ws_cap) return LIBPT_OK;
+    set_error("scratch arena workspace smaller than one triple");
+    return LIBPT_ERR_NOMEM;
+  }
   want = std::max(std::min<int64_t>(want, (int64_t)(p->ws_budget / 8)), biggest);
   const size_t tri = std::max<size_t>(
       1, std::min<size_t>({(size_t)4096, ents.size(),
                            (size_t)(want / std::max<int64_t>(p->ws_stride_min, 1))}));
   if (want <= p->ws_cap && tri <= p->tri_cap) return LIBPT_OK;
-  if (p->arena) {
-    set_error("scratch arena workspace exceeded");
-    return LIBPT_ERR_NOMEM;
-  }
   CK(cudaStreamSynchronize(p->st));
   for (void **q : {(void **)&p->ws, (void **)&p->partials, (void **)&p->d_desc}) {
     if (!*q) continue;
@@ -1447,9 +1448,10 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       const size_t slack = 3 * 256 + d0;
       const size_t left =
           p->arena_size > used + slack ? p->arena_size - used - slack : 0;
-      size_t nb = std::min<size_t>({left / per, (size_t)4096,
-                                    p->queue.size()});
-      if (arena_nb) nb = std::min(nb, arena_nb);
+      // a requested round size is taken as is (the allocations below fail
+      // if the arena cannot hold it); else as many triples as fit
+      const size_t nb = std::min<size_t>(
+          {arena_nb ? arena_nb : left / per, (size_t)4096, p->queue.size()});
       if (nb == 0) {
         set_error("scratch arena too small for one triple");
         r = LIBPT_ERR_NOMEM;

@@ -29,6 +29,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -104,6 +105,7 @@ struct Solve {
   double remaining = 0.0;        // reference flops left to schedule
   bool done = false;
   int status = LIBPT_OK;
+  std::string error;             // message of a failure
   double energy = 0.0;
 };
 
@@ -152,9 +154,10 @@ namespace ptb {
 namespace {
 
 void finish(libpt_server *S, const std::shared_ptr<Solve> &s, int status) {
-  // caller holds S->mu
+  // caller holds S->mu; the message is this thread's last error
   s->done = true;
   s->status = status;
+  if (status != LIBPT_OK) s->error = last_error();
   s->t_done = now_s();
   if (status == LIBPT_OK)
     ++S->st.completed;
@@ -252,6 +255,8 @@ void admit_loop(libpt_server *S) {
 void complete(libpt_server *S, const std::shared_ptr<Solve> &s, bool err) {
   double e = 0.0;
   int r = err ? LIBPT_ERR_TIMEOUT : LIBPT_OK;
+  if (err) set_error("libpt_server: a device-side wait of the solve's round "
+                     "exceeded its time limit, or the round failed to launch");
   if (!r) r = plan_energy(s->plan, nullptr, 0, &e, S->read_st);
   plan_destroy(s->plan);
   std::lock_guard<std::mutex> lk(S->mu);
@@ -543,6 +548,7 @@ LIBPT_API int libpt_server_wait(libpt_server *S, uint64_t ticket,
     return LIBPT_ERR_TIMEOUT;
   if (energy) *energy = s->energy;
   if (latency_s) *latency_s = s->t_done - s->t_submit;
+  if (s->status != LIBPT_OK) set_error(s->error);
   return s->status;
 }
 
