@@ -70,6 +70,11 @@ def parse():
                          "the headline value")
     ap.add_argument("--slices", type=int, default=6,
                     help="emulated FP64 digit slices (4..7)")
+    ap.add_argument("--serve-requests", type=int, default=40,
+                    help="requests of the served stream (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=20.0,
+                    help="Poisson arrival rate of the served stream (req/s)")
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     return ap.parse_args()
 
 
@@ -381,6 +386,10 @@ def run_ours(args, d):
                    workload=f"libpt_rpt(o={O_E2E}, v={args.v}) host arrays, "
                             "full solve")
 
+    serving = None
+    if args.serve_requests > 0:
+        serving = run_serving(args, torch, gpu_id)
+
     cpu = None
     if not args.no_cpu and d.world == 1 and d.rank == 0:
         try:
@@ -420,7 +429,7 @@ def run_ours(args, d):
                           launches=stats["gemm_launches"],
                           epilogue_ms_share=stats["epi_ms"] /
                           max(secs * 1e3, 1e-9)),
-            cpu_baseline=cpu, e2e=e2e, clocks=clk,
+            cpu_baseline=cpu, e2e=e2e, clocks=clk, serving=serving,
             gpu_launches=stats["launches"],
             energy_sample=energy_sample, setup_seconds=t_gen)
         for name, Rr in runs.items():
@@ -438,6 +447,100 @@ def run_ours(args, d):
                 plan_seconds=Rr["plan_seconds"], clocks=Rr["clk"])
         print(json.dumps(line))
     d.close()
+
+
+def serve_stream(n, rate, seed):
+    """The served workload: restricted (T) requests with o ~ U{4..24},
+    v = round(o * U[6, 12]), Poisson arrivals at `rate` per second, half
+    FP64 and half emulated FP64, one input seed per request."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    reqs = []
+    for i in range(n):
+        o = int(rng.integers(4, 25))
+        v = int(round(o * rng.uniform(6.0, 12.0)))
+        reqs.append(dict(o=o, v=v, seed=10_000 + i, emu=bool(i % 2),
+                         arrival=float(t[i] - t[0])))
+    return reqs
+
+
+def percentile(x, q):
+    return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+
+def run_serving(args, torch, gpu_id):
+    """Served stream through the continuous-batching server (pt_serve.h):
+    each request's inputs are generated on the device when it arrives and
+    submitted; latency runs from submission to its energy.  Beside it, the
+    same requests as one-at-a-time FP64 solves (libpt plan per request,
+    FIFO at the same arrival times, queueing computed from the measured
+    service times)."""
+    from libpt_b200 import ffi, synth
+    reqs = serve_stream(args.serve_requests, args.serve_rate, seed=4)
+    emu = ffi.PREC_EMU64 | (args.slices << 8)
+    budget = int(args.serve_budget_gb * (1 << 30))
+    free = torch.cuda.mem_get_info()[0]
+    # room beside the pool for arriving requests' inputs until admission
+    budget = min(budget, int(free - (24 << 30)))
+    flops = 0.0
+    srv = ffi.Server(mem_budget=budget)
+    clocks = Clocks(gpu_id)
+    clocks.start()
+    t0 = time.perf_counter()
+    tickets = []
+    for r in reqs:
+        while time.perf_counter() - t0 < r["arrival"]:
+            time.sleep(0.0005)
+        srv.release_inputs()            # inputs already resident in the pool
+        meta, tens = synth.rpt_case_device(r["o"], r["v"], seed=r["seed"])
+        torch.cuda.synchronize()
+        tickets.append(srv.submit(meta, tensors=tens,
+                                  precision=emu if r["emu"] else 0))
+        del tens
+        flops += rpt_flops(r["o"], r["v"])
+    lat, energies = [], []
+    for tk in tickets:
+        e, l = srv.wait(tk)
+        lat.append(l)
+        energies.append(e)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    st = srv.stats()
+    srv.close()
+    torch.cuda.empty_cache()
+    # one-at-a-time FP64 solves of the same requests
+    service = []
+    for r in reqs:
+        meta, tens = synth.rpt_case_device(r["o"], r["v"], seed=r["seed"])
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        p = ffi.Plan(meta, tens)
+        p.run()
+        p.energy()
+        p.close()
+        service.append(time.perf_counter() - a)
+        del tens
+    torch.cuda.empty_cache()
+    done, blat = 0.0, []
+    for r, sv in zip(reqs, service):
+        done = max(done, r["arrival"]) + sv
+        blat.append(done - r["arrival"])
+    return dict(
+        workload=f"{len(reqs)} restricted (T) requests, o~U{{4..24}}, "
+                 f"v=round(o*U[6,12]), Poisson {args.serve_rate:g} req/s, "
+                 f"half FP64 / half emulated FP64 ({args.slices} slices), "
+                 "inputs generated on the device at arrival",
+        solves_per_s=len(reqs) / wall, p50_s=percentile(lat, 50),
+        p99_s=percentile(lat, 99), tflops=flops / wall / 1e12,
+        rounds=st["rounds"], graph_rounds=st["graph_rounds"],
+        max_resident=st["max_resident"],
+        peak_pool_gb=st["peak_bytes_in_use"] / 2**30,
+        pool_gb=st["pool_bytes"] / 2**30, clocks=clk,
+        one_at_a_time_fp64=dict(
+            solves_per_s=len(reqs) / done, p50_s=percentile(blat, 50),
+            p99_s=percentile(blat, 99),
+            note="sequential FP64 plan per request, FIFO queue at the same "
+                 "arrivals (service times measured)"))
 
 
 def main():

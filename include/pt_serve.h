@@ -51,8 +51,9 @@ int libpt_server_create(size_t mem_budget, int max_active,
 
 /* Queues a solve.  args: the pt.h arguments of `kind` in the reference's
  * order (host pointers when host_inputs, else device pointers); they must
- * stay valid and unchanged until libpt_server_wait / _poll report the
- * solve done.  *ticket identifies it.  Ownership stays with the caller. */
+ * stay valid and unchanged until libpt_server_inputs_released reports them
+ * released (at the latest when libpt_server_wait reports the solve done).
+ * *ticket identifies it.  Ownership stays with the caller. */
 int libpt_server_submit(libpt_server *s, int kind, size_t oa, size_t va,
                         size_t ob, size_t vb, const void *const *args,
                         int dtype, int precision, int host_inputs,
@@ -64,6 +65,12 @@ int libpt_server_submit(libpt_server *s, int kind, size_t oa, size_t va,
  * error that ended it).  LIBPT_ERR_TIMEOUT if it is still running. */
 int libpt_server_wait(libpt_server *s, uint64_t ticket, double timeout_s,
                       double *energy, double *latency_s);
+
+/* Non-blocking: *released = 1 once the server no longer reads the solve's
+ * arguments (its operands are resident in the pool, or it ended), so the
+ * caller may free or reuse them before the solve completes. */
+int libpt_server_inputs_released(libpt_server *s, uint64_t ticket,
+                                 int *released);
 
 /* Counters of the server's life so far. */
 typedef struct {

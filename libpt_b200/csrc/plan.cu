@@ -1043,8 +1043,11 @@ int plan_append(libpt_plan *p, const int64_t *ents, size_t n, PlanCursor &cur,
   for (size_t t = 0; t < n; ++t) {
     const int4 q = p->queue[ents[t]];
     SpinCase &c = p->cases[q.x];
-    if (cur.triples >= p->tri_cap || cur.ws + c.ws_stride > p->ws_cap ||
-        cur.part + c.ntiles > p->part_cap)
+    const int64_t wend = cur.ws_end >= 0 ? cur.ws_end : p->ws_cap;
+    const int64_t pend = cur.part_end >= 0 ? cur.part_end : p->part_cap;
+    const size_t tend = cur.tri_end ? cur.tri_end : p->tri_cap;
+    if (cur.triples >= tend || cur.ws + c.ws_stride > wend ||
+        cur.part + c.ntiles > pend)
       break;   // the round is full for this plan
     const int ijk[3] = {q.y, q.z, q.w};
     double *ws = p->ws + cur.ws;

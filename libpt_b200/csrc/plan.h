@@ -191,10 +191,14 @@ int dmma_map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R,
 int dmma_map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld,
                int64_t K, int64_t P);
 int plan_run(libpt_plan *p, const int64_t *idx, size_t n);
-// Where the next triple of a plan goes in its round resources.
+// Where the next triple of a plan goes in its round resources, and the end
+// of the region this round may use (negative / zero: the plan's capacity),
+// so two rounds of one plan can be in flight in disjoint halves.
 struct PlanCursor {
   int64_t ws = 0, part = 0;
   size_t triples = 0;
+  int64_t ws_end = -1, part_end = -1;
+  size_t tri_end = 0;
 };
 // Appends queue entries ents[0..n) of plan p to a round while they fit the
 // plan's round resources (from cur on); *taken = entries appended.

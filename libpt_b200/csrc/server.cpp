@@ -102,8 +102,11 @@ struct Solve {
   libpt_plan *plan = nullptr;
   size_t total = 0, next = 0;    // queue entries, next to schedule
   int inflight = 0;              // rounds holding its triples, not retired
+  int halves = 1;                // 2: its round resources are split so two
+  int half = 0;                  // rounds can be in flight (next half)
   double remaining = 0.0;        // reference flops left to schedule
   bool done = false;
+  bool consumed = false;         // inputs copied (or the solve ended)
   int status = LIBPT_OK;
   std::string error;             // message of a failure
   double energy = 0.0;
@@ -120,7 +123,7 @@ constexpr double ROUND_FLOPS = 1.5e12;
 constexpr double GRAPH_FLOPS = 5e10;
 constexpr size_t ROUND_TRIPLES = 8192;
 constexpr size_t JOBS_PER_TRIPLE = 6;
-constexpr size_t WS_TARGET = (size_t)2 << 30;
+constexpr size_t WS_TARGET = (size_t)4 << 30;   // per round, per solve
 
 }  // namespace
 }  // namespace ptb
@@ -156,6 +159,7 @@ namespace {
 void finish(libpt_server *S, const std::shared_ptr<Solve> &s, int status) {
   // caller holds S->mu; the message is this thread's last error
   s->done = true;
+  s->consumed = true;
   s->status = status;
   if (status != LIBPT_OK) s->error = last_error();
   s->t_done = now_s();
@@ -166,8 +170,28 @@ void finish(libpt_server *S, const std::shared_ptr<Solve> &s, int status) {
   S->cv_done.notify_all();
 }
 
+// Triples in the queue of a solve (src/pt.c:208-221, 331-344): i<j<k per
+// same-spin space, i<j (x) k per mixed-spin pair of spaces.
+size_t queue_length(int kind, size_t oa, size_t va, size_t ob, size_t vb) {
+  const bool unr = kind == 1 || kind == 3;
+  if (!unr) {
+    ob = oa;
+    vb = va;
+  }
+  auto c3 = [](size_t o, size_t v) { return v ? o * (o - 1) * (o - 2) / 6 : 0; };
+  auto c2k = [](size_t o1, size_t v1, size_t o2, size_t v2) {
+    return (v1 && v2 && o2) ? o1 * (o1 - 1) / 2 * o2 : 0;
+  };
+  if (oa < 2 && ob < 2) return 0;
+  size_t n = (oa >= 3 ? c3(oa, va) : 0) + (oa >= 2 ? c2k(oa, va, ob, vb) : 0);
+  if (unr)
+    n += (ob >= 3 ? c3(ob, vb) : 0) + (ob >= 2 ? c2k(ob, vb, oa, va) : 0);
+  return n;
+}
+
 // Round triples a solve may hold: its whole queue when that fits the
-// workspace target, else what the target holds (at least one).
+// workspace target, else what the target holds (at least one), twice when
+// its queue needs more than one round (two rounds in flight).
 int size_solve(Solve &s) {
   const size_t f1 = plan_footprint(s.kind, s.oa, s.va, s.ob, s.vb, s.dtype,
                                    s.precision, s.host, 1);
@@ -177,9 +201,11 @@ int size_solve(Solve &s) {
   const size_t per = f2 > f1 ? f2 - f1 : 1;
   size_t nb = std::max<size_t>(1, WS_TARGET / per);
   nb = std::min(nb, ROUND_TRIPLES);
-  s.nb = nb;
+  const size_t nq = queue_length(s.kind, s.oa, s.va, s.ob, s.vb);
+  s.halves = nq > nb ? 2 : 1;
+  s.nb = std::min(nb * s.halves, std::max<size_t>(nq, 1));
   s.bytes = plan_footprint(s.kind, s.oa, s.va, s.ob, s.vb, s.dtype,
-                           s.precision, s.host, nb);
+                           s.precision, s.host, s.nb);
   return s.bytes ? LIBPT_OK : LIBPT_ERR_ARG;
 }
 
@@ -230,6 +256,7 @@ void admit_loop(libpt_server *S) {
       continue;
     }
     s->plan = p;
+    s->consumed = true;   // plan_create synchronized its uploads
     s->total = p->queue.size();
     s->remaining = plan_flops(p, 0, (int64_t)s->total);
     --S->admitting;
@@ -306,7 +333,7 @@ void run_loop(libpt_server *S) {
     {
       std::unique_lock<std::mutex> lk(S->mu);
       for (auto &s : S->resident)
-        if (s->next < s->total && s->inflight == 0) cand.push_back(s);
+        if (s->next < s->total && s->inflight < s->halves) cand.push_back(s);
       if (cand.empty() && S->inflight.empty()) {
         if (S->stop && S->pending.empty() && S->admitting == 0 &&
             S->resident.empty())
@@ -349,12 +376,22 @@ void run_loop(libpt_server *S) {
         if (round.gemm_flops + f >= ROUND_FLOPS) break;
       }
       PlanCursor cur;
+      if (s->halves == 2) {   // alternate halves of its round resources
+        const int h = s->half;
+        cur.ws = h ? p->ws_cap / 2 : 0;
+        cur.ws_end = h ? p->ws_cap : p->ws_cap / 2;
+        cur.part = h ? p->part_cap / 2 : 0;
+        cur.part_end = h ? p->part_cap : p->part_cap / 2;
+        cur.triples = h ? p->tri_cap / 2 : 0;
+        cur.tri_end = h ? p->tri_cap : p->tri_cap / 2;
+      }
       size_t taken = 0;
       if (plan_append(p, ents.data(), ents.size(), cur, round, &taken) ||
           taken == 0)
         continue;
       s->remaining -= plan_flops(p, (int64_t)s->next, (int64_t)taken);
       s->next += taken;
+      s->half ^= 1;
       rr.solves.push_back(s);
     }
     if (rr.solves.empty()) {
@@ -550,6 +587,19 @@ LIBPT_API int libpt_server_wait(libpt_server *S, uint64_t ticket,
   if (latency_s) *latency_s = s->t_done - s->t_submit;
   if (s->status != LIBPT_OK) set_error(s->error);
   return s->status;
+}
+
+LIBPT_API int libpt_server_inputs_released(libpt_server *S, uint64_t ticket,
+                                           int *released) {
+  if (!S || !released) return LIBPT_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->by_id.find(ticket);
+  if (it == S->by_id.end()) {
+    set_error("libpt_server_inputs_released: unknown ticket");
+    return LIBPT_ERR_ARG;
+  }
+  *released = it->second->consumed ? 1 : 0;
+  return LIBPT_OK;
 }
 
 LIBPT_API int libpt_server_stats_get(libpt_server *S, libpt_server_stats *out) {

@@ -104,6 +104,9 @@ def lib():
                                       [ctypes.POINTER(ctypes.c_uint64)])
     L.libpt_server_wait.restype = ctypes.c_int
     L.libpt_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, dp, dp]
+    L.libpt_server_inputs_released.restype = ctypes.c_int
+    L.libpt_server_inputs_released.argtypes = [vp, ctypes.c_uint64,
+                                               ctypes.POINTER(ctypes.c_int)]
     L.libpt_server_stats_get.restype = ctypes.c_int
     L.libpt_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
     L.libpt_server_destroy.restype = ctypes.c_int
@@ -240,6 +243,17 @@ class Server:
             self._keep.pop(ticket, None)
         check(code)
         return e.value, lat.value
+
+    def release_inputs(self):
+        """Drops the references to inputs the server no longer reads;
+        returns how many solves still hold theirs."""
+        for t in list(self._keep):
+            r = ctypes.c_int(0)
+            check(lib().libpt_server_inputs_released(self.h, t,
+                                                     ctypes.byref(r)))
+            if r.value:
+                del self._keep[t]
+        return len(self._keep)
 
     def stats(self):
         st = ServerStats()
