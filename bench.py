@@ -75,6 +75,10 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=20.0,
                     help="Poisson arrival rate of the served stream (req/s)")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the precision table (unrestricted (T) and (fT))")
+    ap.add_argument("--accuracy-rft", action="store_true",
+                    help="add restricted (fT) o=30 v=300 to the table (~2 min)")
     return ap.parse_args()
 
 
@@ -389,6 +393,9 @@ def run_ours(args, d):
     serving = None
     if args.serve_requests > 0:
         serving = run_serving(args, torch, gpu_id)
+    accuracy = None
+    if not args.no_accuracy:
+        accuracy = run_accuracy(args, torch)
 
     cpu = None
     if not args.no_cpu and d.world == 1 and d.rank == 0:
@@ -430,6 +437,7 @@ def run_ours(args, d):
                           epilogue_ms_share=stats["epi_ms"] /
                           max(secs * 1e3, 1e-9)),
             cpu_baseline=cpu, e2e=e2e, clocks=clk, serving=serving,
+            precision_table=accuracy,
             gpu_launches=stats["launches"],
             energy_sample=energy_sample, setup_seconds=t_gen)
         for name, Rr in runs.items():
@@ -541,6 +549,55 @@ def run_serving(args, torch, gpu_id):
             p99_s=percentile(blat, 99),
             note="sequential FP64 plan per request, FIFO queue at the same "
                  "arrivals (service times measured)"))
+
+
+def run_accuracy(args, torch):
+    """Full solves of unrestricted (T) oa=20 va=180 ob=18 vb=182 and
+    unrestricted (fT) o=15 v=150 (spin blocks 15/150 each), inputs generated
+    on the device, in every precision form: FP64 (DMMA), emulated FP64 with
+    4-7 INT8 slices, and 3xTF32 on the FP32 inputs.  |dE| against the FP64
+    path (the FP64 path matches the reference FP64 build to <= 1e-12 |E| in
+    the parity tests; the CPU reference itself would need ~10 min here).
+    Seconds exclude plan creation (reported apart)."""
+    from libpt_b200 import ffi, synth
+    cases = [("upt", (20, 180, 18, 182)), ("uft", (15, 150, 15, 150))]
+    if args.accuracy_rft:
+        cases.append(("rft", (30, 300)))
+    forms = [("fp64", ffi.PREC_FP64, False)]
+    forms += [(f"emu64_s{s}", ffi.PREC_EMU64 | (s << 8), False)
+              for s in (4, 5, 6, 7)]
+    forms += [("emu64_auto", ffi.PREC_EMU64, False)]   # S chosen for 1 uEh
+    forms += [("tf32x3", ffi.PREC_TF32X3, True)]
+    rows = []
+    for kind, sz in cases:
+        meta, tens = synth.case_device(kind, *sz, seed=7)
+        res = {}
+        for name, prec, mp in forms:
+            src = {k: x.float() for k, x in tens.items()} if mp else tens
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p = ffi.Plan(meta, src, mp=mp, precision=prec)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            p.run()
+            e = p.energy()
+            t2 = time.perf_counter()
+            fl = p.flops()
+            sl = p.slices or None
+            p.close()
+            del src
+            res[name] = dict(seconds=t2 - t1, plan_seconds=t1 - t0,
+                             tflops=fl / (t2 - t1) / 1e12, energy=e,
+                             slices=sl)
+        e64 = res["fp64"]["energy"]
+        for name, r in res.items():
+            r["dE_uEh"] = abs(r["energy"] - e64) * 1e6
+            r["dE_rel"] = abs(r["energy"] - e64) / abs(e64) if e64 else None
+            r["speedup_vs_fp64"] = res["fp64"]["seconds"] / r["seconds"]
+        rows.append(dict(kind=kind, sizes=list(sz), flops=fl, forms=res))
+        del tens
+        torch.cuda.empty_cache()
+    return rows
 
 
 def main():

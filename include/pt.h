@@ -110,8 +110,12 @@ const char *libpt_last_error(void);
                                  (power-of-two scale per row / column), exact
                                  INT32 accumulation of the S(S+1)/2 leading
                                  digit products on tcgen05 INT8 tensor cores.
-                                 S = 6 by default; LIBPT_PREC_EMU64 | (S << 8)
-                                 selects S in [4, 7]                          */
+                                 LIBPT_PREC_EMU64 | (S << 8) fixes S in
+                                 [4, 7]; S = 0 lets the plan choose the
+                                 smallest S whose error bound, estimated on a
+                                 sample of triples against 7 slices, is under
+                                 LIBPT_EMU_TOL / 2 (environment, Eh; default
+                                 1e-6, the north star's 1 uEh)               */
 
 /* Built-in self-test of a contraction kernel: C = A B1 - A B2 on random
  * m x k and k x n operands, against an FP64 reference computed on the device;
@@ -224,6 +228,9 @@ int libpt_plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     libpt_plan **out);
 /* Number of entries of the triples queue. */
 int64_t libpt_plan_queue_length(const libpt_plan *plan);
+/* Digit slices an emulated-FP64 plan runs with (its choice when created
+ * with S = 0), 0 for the other precision modes. */
+int libpt_plan_slices(const libpt_plan *plan);
 /* Algorithmic flops of queue entries [first, first+n): twice the
  * multiply-adds of the reference's own contractions for those triples. */
 double libpt_plan_flops(const libpt_plan *plan, int64_t first, int64_t n);

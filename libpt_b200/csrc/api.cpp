@@ -274,6 +274,10 @@ LIBPT_API int64_t libpt_plan_queue_length(const libpt_plan *plan) {
   return plan ? (int64_t)plan->queue.size() : -1;
 }
 
+LIBPT_API int libpt_plan_slices(const libpt_plan *plan) {
+  return plan && plan->precision == LIBPT_PREC_EMU64 ? plan->slices : 0;
+}
+
 LIBPT_API double libpt_plan_flops(const libpt_plan *plan, int64_t first,
                                   int64_t n) {
   return plan ? ptb::plan_flops(plan, first, n) : 0.0;

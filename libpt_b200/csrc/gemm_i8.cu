@@ -8,7 +8,9 @@
 //     acc_w = sum over digit pairs p + q = w (w <= S-1) of dA_p dB_q,
 // each acc_w an exact INT32 sum in its own TMEM accumulator (S accumulators
 // of BN columns; S * BN <= 512).  Subtracted segments read the negated
-// digit planes (A planes S..2S-1), so all products accumulate with +.
+// digit planes (stored after the digit planes; GemmSeg::neg holds their
+// first plane), so all products accumulate with +.  The kernel may use the
+// first S of more stored planes (the digits of a shorter decomposition).
 //
 // Tile variants (BN columns, KC = 32 or 64 bytes of K per pipeline stage):
 // an M=128 INT8 MMA reads (128 + BN) * 32 bytes of shared memory per
@@ -185,7 +187,7 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
       const int nseg = job.nseg;
       for (int s = 0; s < nseg && ok; ++s) {
         const GemmSeg sg = job.seg[s];
-        const int aoff = sg.neg ? S : 0;
+        const int aoff = sg.neg;   // first negated digit plane, or 0
         const CUtensorMap *am = ms.get(job, sg.amap);
         const CUtensorMap *bm = ms.get(job, sg.bmap);
         for (int ks = 0; ks < sg.ksteps; ++ks) {

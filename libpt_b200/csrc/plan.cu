@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -836,8 +837,9 @@ int i8_encode(libpt_plan *p, SpinCase &c) {
     const int r =
         d.role == 0
             ? i8_map_a(&c.tcmaps.m[i], c.i8pl[i], d.K, d.R, d.Q, d.P,
-                       p->slices)
-            : i8_map_b(&c.tcmaps.m[i], c.i8pl[i], d.K, d.N, d.P, p->slices,
+                       p->slices_store)
+            : i8_map_b(&c.tcmaps.m[i], c.i8pl[i], d.K, d.N, d.P,
+                       p->slices_store,
                        p->i8tile.bn);
     if (r) return r;
   }
@@ -845,7 +847,7 @@ int i8_encode(libpt_plan *p, SpinCase &c) {
 }
 
 int i8_planes(libpt_plan *p, SpinCase &c) {
-  const int S = p->slices;
+  const int S = p->slices_store;
   for (int i = 0; i < MAX_MAPS; ++i) {
     const OpDesc &d = c.opd[i];
     if (d.role < 0) continue;
@@ -1082,7 +1084,9 @@ int plan_append(libpt_plan *p, const int64_t *ents, size_t n, PlanCursor &cur,
         GemmSeg &gs = g.seg[s];
         gs.amap = (int16_t)(tc ? 2 * st.amap : st.amap);
         gs.bmap = (int16_t)(tc ? 2 * st.bmap : st.bmap);
-        gs.neg = st.neg;
+        // INT8: a subtracted segment reads the negated digit planes, stored
+        // after the slices_store digit planes
+        gs.neg = (int16_t)(st.neg ? (i8 ? p->slices_store : 1) : 0);
         gs.a_q = ijk[st.aq];
         gs.a_p = ijk[st.ap];
         if (i8) {   // INT8 A views merge (Q, P) into one coordinate
@@ -1172,6 +1176,68 @@ int set_bm(SpinCase &c, int bm) {
     if (d.role == 0)
       if (int r = map_a(&c.maps.m[i], d.src, d.K, d.R, d.Q, d.P, bm)) return r;
   }
+  return LIBPT_OK;
+}
+
+// Emulated FP64 with the slice count left to the library: the digit planes
+// are built with the most slices (7), whose first S planes are exactly the
+// S-slice decomposition (digits come from the running remainder), so any
+// S <= 7 runs on them.  A sample of up to 16 triples spread over the queue
+// is evaluated with 7 slices and with 4, 5, 6; the error of the whole solve
+// with S slices is bounded by (queue / sample) * sum over the sample of
+// |e_S - e_7| (no cancellation assumed), and the smallest S whose bound is
+// under half the tolerance (LIBPT_EMU_TOL, default 1e-6 Eh) is kept.
+int choose_slices(libpt_plan *p) {
+  const size_t N = p->queue.size();
+  if (!N) return LIBPT_OK;
+  const size_t n = std::min<size_t>(N, 16);
+  std::vector<int64_t> ents(n);
+  for (size_t t = 0; t < n; ++t) ents[t] = (int64_t)(t * N / n);
+  std::vector<double> slots(N + 1), ref(n);
+  auto run_with = [&](int S, std::vector<double> &out) -> int {
+    const I8Tile *tiles = nullptr;
+    if (i8_tiles(S, &tiles) <= 0) return LIBPT_ERR_ARG;
+    p->slices = S;
+    p->i8tile = tiles[0];
+    for (SpinCase &c : p->cases)
+      if (c.count)
+        if (int r = i8_encode(p, c)) return r;
+    if (int r = upload_views(p)) return r;
+    if (int r = run_entries(p, ents)) return r;
+    CK(cudaMemcpyAsync(slots.data(), p->e_slot, (N + 1) * 8,
+                       cudaMemcpyDeviceToHost, p->st));
+    CK(cudaStreamSynchronize(p->st));
+    out.resize(n);
+    for (size_t t = 0; t < n; ++t) out[t] = slots[(size_t)ents[t]];
+    return LIBPT_OK;
+  };
+  if (int r = run_with(TC_S_MAX, ref)) return r;
+  int chosen = TC_S_MAX;
+  std::vector<double> e;
+  for (int S = TC_S_MIN; S < TC_S_MAX; ++S) {
+    if (int r = run_with(S, e)) return r;
+    double bound = 0.0;
+    for (size_t t = 0; t < n; ++t) bound += std::fabs(e[t] - ref[t]);
+    bound *= p->factor * (double)N / (double)n;
+    if (tune_verbose())
+      std::fprintf(stderr, "libpt slices: S=%d error bound %.3e Eh (target %.1e)\n",
+                   S, bound, p->emu_tol);
+    if (bound <= 0.5 * p->emu_tol) {
+      chosen = S;
+      break;
+    }
+  }
+  const I8Tile *tiles = nullptr;
+  i8_tiles(chosen, &tiles);
+  p->slices = chosen;
+  p->i8tile = tiles[0];
+  for (SpinCase &c : p->cases)
+    if (c.count)
+      if (int r = i8_encode(p, c)) return r;
+  if (int r = upload_views(p)) return r;
+  CK(cudaMemsetAsync(p->e_slot, 0, (N + 1) * 8, p->st));
+  CK(cudaStreamSynchronize(p->st));
+  p->launches = 0;
   return LIBPT_OK;
 }
 
@@ -1304,7 +1370,8 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     set_error("libpt_plan_create: unknown precision mode");
     return LIBPT_ERR_ARG;
   }
-  if (slices == 0) slices = 6;
+  const bool auto_slices = slices == 0;
+  if (auto_slices) slices = TC_S_MAX;   // chosen after the planes exist
   if (slices < TC_S_MIN || slices > TC_S_MAX) {
     set_error("libpt_plan_create: emulated FP64 takes 4 to 7 slices");
     return LIBPT_ERR_ARG;
@@ -1336,6 +1403,12 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
   p->dtype = dtype;
   p->precision = precision;
   p->slices = slices;
+  p->slices_store = slices;
+  p->slices_auto = auto_slices && precision == LIBPT_PREC_EMU64;
+  if (const char *t = std::getenv("LIBPT_EMU_TOL")) {
+    const double v = std::atof(t);
+    if (v > 0) p->emu_tol = v;
+  }
   {
     const I8Tile *t = nullptr;
     if (i8_tiles(slices, &t) > 0) p->i8tile = t[0];   // widest tile
@@ -1481,6 +1554,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     p->ws_budget = std::min<size_t>(std::max<size_t>(fr / 2, (size_t)64 << 20),
                                     (size_t)16 << 30);
   } while (0);
+  if (!r && !g_dry && p->slices_auto) r = choose_slices(p);
   if (!r && !g_dry) r = autotune(p);
   if (r) {
     plan_destroy(p);

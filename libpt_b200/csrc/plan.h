@@ -146,7 +146,10 @@ struct libpt_plan {
   // tensor-core planes, keyed by (source block, role)
   std::vector<std::pair<std::pair<const double *, int>, ptb::Planes>> planes;
   // emulated FP64: digit planes per (source block, role), scale families
-  int slices = 6;
+  int slices = 6;                       // digit planes the kernels use
+  int slices_store = 6;                 // digit planes stored (>= slices)
+  bool slices_auto = false;             // choose slices for emu_tol
+  double emu_tol = 1e-6;                // |dE| target of the choice (Eh)
   ptb::I8Tile i8tile{64, 32};           // emulated FP64 tile variant
   std::vector<std::pair<std::pair<const double *, int>, signed char *>> i8planes;
   std::vector<ptb::Family> fams;

@@ -220,7 +220,7 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
     for (int s2 = 0; s2 < 2; ++s2) {
       job.seg[s2].amap = 0;
       job.seg[s2].bmap = (int16_t)(1 + s2);
-      job.seg[s2].neg = (int16_t)s2;
+      job.seg[s2].neg = (int16_t)(s2 ? S : 0);   // negated planes from S on
       job.seg[s2].ksteps = (k + kc - 1) / kc;
     }
     publish(&tcmaps_scratch(), sizeof(TcMapSet));

@@ -24,7 +24,7 @@ ERRORS = {1: "LIBPT_ERR_ARG", 2: "LIBPT_ERR_NOMEM", 3: "LIBPT_ERR_CUDA",
           4: "LIBPT_ERR_TIMEOUT", 5: "LIBPT_ERR_UNSUPPORTED"}
 PREC_FP64 = 0
 PREC_TF32X3 = 1
-PREC_EMU64 = 2          # | (slices << 8), slices 4..7 (default 6)
+PREC_EMU64 = 2          # | (slices << 8), slices 4..7; 0: chosen for 1 uEh
 
 _lib = None
 
@@ -71,6 +71,8 @@ def lib():
                                     ctypes.c_int, vp, ctypes.POINTER(vp)]
     L.libpt_plan_queue_length.restype = ctypes.c_int64
     L.libpt_plan_queue_length.argtypes = [vp]
+    L.libpt_plan_slices.restype = ctypes.c_int
+    L.libpt_plan_slices.argtypes = [vp]
     L.libpt_plan_flops.restype = ctypes.c_double
     L.libpt_plan_flops.argtypes = [vp, ctypes.c_int64, ctypes.c_int64]
     L.libpt_plan_run.restype = ctypes.c_int
@@ -290,6 +292,7 @@ class Plan:
                                       ctypes.byref(h)))
         self.h = h
         self.n = lib().libpt_plan_queue_length(h)
+        self.slices = lib().libpt_plan_slices(h)
 
     def flops(self, first=0, n=None):
         return lib().libpt_plan_flops(self.h, first,

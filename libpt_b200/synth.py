@@ -249,3 +249,87 @@ def restricted_as_unrestricted(case):
         if n in case:
             out[n] = dup4(case[n], nw)
     return out
+
+
+def case_device(kind, oa, va, ob=None, vb=None, seed=0, fock=0.0,
+                device="cuda"):
+    """Any of the four kinds generated on the GPU with torch (same recipes
+    and distributions as the host generators above, not the same numbers),
+    for the larger accuracy workloads.  Returns (meta, tensors): pt.h-layout
+    float64 CUDA tensors keyed by the pt.h argument names."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    f64 = dict(dtype=torch.float64, device=device)
+    restricted = kind[0] == "r"
+    if restricted:
+        ob, vb = oa, va
+    ob = oa if ob is None else ob
+    vb = va if vb is None else vb
+
+    def normal(shape, std):
+        return torch.randn(shape, generator=g, **f64).mul_(std)
+
+    def energies(o, v):
+        ei = torch.rand(o, generator=g, **f64) * 1.2 - 1.5
+        ea = torch.rand(v, generator=g, **f64) * 2.9 + 0.1
+        return (ei[:, None] - ea[None, :]).reshape(-1)
+
+    def pack(x):
+        v = x.shape[-1]
+        r, c = torch.tril_indices(v, v, -1, device=device)
+        return x.reshape(*x.shape[:-2], v * v).index_select(-1, r * v + c)
+
+    def cat(*blocks):
+        return torch.cat([b.reshape(-1) for b in blocks])
+
+    def oovv_like(std):
+        if restricted:
+            x = normal((oa, oa, va, va), std)
+            ab = 0.5 * (x + x.permute(1, 0, 3, 2))
+            return cat(ab - ab.transpose(2, 3), ab)
+        def same(o, v):
+            x = normal((o, o, v, v), std)
+            x = x - x.transpose(0, 1)
+            return 0.5 * (x - x.transpose(2, 3))
+        ab = normal((oa, ob, va, vb), std)
+        return cat(same(oa, va), ab, same(ob, vb), ab.permute(1, 0, 3, 2))
+
+    def oovo_like(std):
+        if restricted:
+            ab = normal((oa, oa, va, oa), std)
+            return cat(ab - ab.transpose(0, 1), ab)
+        aa = normal((oa, oa, va, oa), std)
+        bb = normal((ob, ob, vb, ob), std)
+        return cat(aa - aa.transpose(0, 1), normal((oa, ob, va, ob), std),
+                   bb - bb.transpose(0, 1), normal((ob, oa, vb, oa), std))
+
+    def ovvv_like(std):
+        def same(o, v):   # one occupied slice at a time (temporaries small)
+            return torch.cat([pack(s - s.transpose(1, 2))
+                              for s in normal((o, v, v, v), std)])
+        if restricted:
+            ab = normal((oa, va, va, va), std)
+            aa = torch.cat([pack(s - s.transpose(1, 2)) for s in ab])
+            return cat(aa, ab)
+        return cat(same(oa, va), normal((oa, vb, va, vb), std),
+                   same(ob, vb), normal((ob, va, vb, va), std))
+
+    nov = oa * va + (0 if restricted else ob * vb)
+    d = energies(oa, va) if restricted else torch.cat([energies(oa, va),
+                                                       energies(ob, vb)])
+    f = normal((nov,), fock) if fock else torch.zeros(nov, **f64)
+    meta = dict(kind=kind, oa=oa, va=va, ob=ob, vb=vb)
+    if kind[1:] == "pt":
+        t = dict(d_ov=d, f_ov=f, t1=normal((nov,), 1e-3),
+                 t2=oovv_like(1e-2), i_oovo=oovo_like(5e-2),
+                 i_oovv=oovv_like(5e-2), i_ovvv=ovvv_like(5e-2))
+    else:
+        omega = float(torch.rand(1, generator=g, **f64) * 0.3 + 0.2)
+        meta["omega"] = omega
+        t = dict(d_ov=d + omega / 3.0, f2_ov=f, l1=normal((nov,), 1e-3),
+                 t2=oovv_like(1e-2), l2=oovv_like(1e-2),
+                 i_oovv=oovv_like(5e-2), i2_t2f2_oovo=oovo_like(5e-2),
+                 i3_ovvv=ovvv_like(5e-2), i6_oovo=oovo_like(5e-2),
+                 i7_ovvv=ovvv_like(5e-2))
+    return meta, {k: x.contiguous() for k, x in t.items()}

@@ -174,7 +174,7 @@ def test_golden_emulated_fp64(name, energies):
     """Emulated FP64 (6 slices) on the golden fixtures: the reference FP64
     value to 1e-12 Eh (measured <= 1e-14)."""
     case = fixtures.load(name)
-    p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64)
+    p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64 | (6 << 8))
     p.run()
     e = p.energy()
     p.close()
@@ -189,9 +189,45 @@ def test_synthetic_emulated_fp64(kind, sz):
     |E| ~ 1e1, 3e-14 Eh on |E| ~ 5e-3)."""
     case = synth.make(kind, *sz, seed=5, fock=1e-3)
     ref = oracle.solve(checker(), case)
-    p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64)
+    p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64 | (6 << 8))
     p.run()
     e = p.energy()
     p.close()
     assert abs(e - ref) <= 1e-6
     assert abs(e - ref) <= 1e-11 * abs(ref) + 1e-13
+
+
+@pytest.mark.parametrize("kind,sz", [("rpt", (8, 64)), ("upt", (5, 21, 4, 23)),
+                                     ("rft", (5, 30)), ("uft", (4, 17, 3, 19)),
+                                     ("rpt", (12, 90))])
+def test_emulated_fp64_chosen_slices_meet_1_uEh(kind, sz):
+    """Slice count left to the plan (S = 0): the chosen S keeps |dE| within
+    the 1 uEh target against the reference FP64 value."""
+    case = synth.make(kind, *sz, seed=6, fock=1e-3)
+    ref = oracle.solve(checker(), case)
+    p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64)
+    p.run()
+    e = p.energy()
+    p.close()
+    assert abs(e - ref) <= 1e-6, (e, ref)
+
+
+def test_emulated_fp64_digit_prefix_equals_fixed_slices():
+    """The first S of 7 stored digit planes are the S-slice decomposition:
+    a plan that chose S from 7-slice planes gives the same energy as a plan
+    built with S slices."""
+    import os
+    case = synth.make("rpt", 6, 40, seed=8, fock=1e-3)
+    os.environ["LIBPT_EMU_TOL"] = "1e3"          # loose: the choice is S = 4
+    try:
+        p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64)
+        p.run()
+        e_auto = p.energy()
+        p.close()
+    finally:
+        del os.environ["LIBPT_EMU_TOL"]
+    q = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64 | (4 << 8))
+    q.run()
+    e4 = q.energy()
+    q.close()
+    assert e_auto == e4
