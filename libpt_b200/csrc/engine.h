@@ -167,6 +167,8 @@ struct EpiArgs {
   int ntiles;             // CTA tiles of one triple
   const int4 *tiles;      // aaa: (a0, b0, c0); aab: (a0, b0, 0) block pairs
   int ctiles;             // aab: number of c blocks
+  int has_f;              // f_ov / f2_ov has a nonzero entry (else its
+                          // disconnected-term products are skipped)
 };
 
 // One triple of an epilogue launch.

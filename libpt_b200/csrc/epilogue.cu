@@ -32,6 +32,10 @@ __device__ __forceinline__ int64_t pairidx(int p, int q) {
   return (int64_t)p * (p - 1) / 2 + q;
 }
 
+__device__ __forceinline__ int pair32(int p, int q) {
+  return p * (p - 1) / 2 + q;
+}
+
 // Fixed-order block reduction of one double per thread.
 __device__ double block_sum(double x) {
   __shared__ double red[EPI_THREADS / 32];
@@ -49,9 +53,24 @@ __device__ double block_sum(double x) {
 // ---------------------------------------------------------------- aaa ----
 
 // Thread layout of both epilogues: warp w handles a = a0 + w, lane l handles
-// c = c0 + l, and each thread walks the tile's 8 values of b.  All loads a
-// thread needs are issued before they are used (unrolled, branch-free with
-// clamped indices and a validity mask), so many requests are in flight.
+// c = c0 + l, and each thread walks the tile's 8 values of b (unrolled,
+// branch-free with clamped indices and a validity mask, so the loads of
+// several b are in flight together).
+
+// 8-byte asynchronous global -> shared copy; ok == false writes 0.0 (the
+// source is not read: src-size 0 zero-fills the destination).
+__device__ __forceinline__ void cp_async8(double *dst, const double *src,
+                                          bool ok) {
+  asm volatile(
+      "cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(ok ? 8 : 0)
+      : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::
+                   : "memory");
+}
 
 // Copies an item's case arguments into shared memory (all threads).
 __device__ __forceinline__ void load_args(EpiArgs &dst, const EpiArgs *src) {
@@ -88,34 +107,28 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
   const int a0 = tl.x, b0 = tl.y, c0 = tl.z;
   const int i = item.i, j = item.j, k = item.k;
   const int v = p.va, o = p.oa;
+  const bool has_f = p.has_f != 0;
+  const int g1l = (int)p.g1_ld_aa, g2l = (int)p.g2_ld_aa;
   const double *base = item.ws;
   const double *T = base + p.offL[0];
   const double *R = FT ? base + p.offR[0] : nullptr;
   const int64_t ld = p.ld[0];
+  const int ldi = (int)ld;
 
-  {
-    double vt[NIT], vr[NIT];
+  // stage T[c][pair(a,b)] asynchronously; its wait comes after the loads
+  // of the per-thread operands below, so both latencies overlap
 #pragma unroll
-    for (int it = 0; it < NIT; ++it) {
-      const int e = threadIdx.x + it * EPI_THREADS;
-      const int a_ = e / (EPI_C * EPI_B), c_ = (e / EPI_B) % EPI_C,
-                b_ = e % EPI_B;
-      const int a = a0 + a_, b = b0 + b_, c = c0 + c_;
-      const bool ok = a < v && b < a && c < b;
-      const int64_t off = ok ? (int64_t)c * ld + pairidx(a, b) : 0;
-      vt[it] = ok ? T[off] : 0.0;
-      vr[it] = (FT && ok) ? R[off] : 0.0;
-    }
-#pragma unroll
-    for (int it = 0; it < NIT; ++it) {
-      const int e = threadIdx.x + it * EPI_THREADS;
-      const int a_ = e / (EPI_C * EPI_B), c_ = (e / EPI_B) % EPI_C,
-                b_ = e % EPI_B;
-      s3[(a_ * EPI_B + b_) * EPI_CS + c_] = vt[it];
-      if (FT) s3[S + (a_ * EPI_B + b_) * EPI_CS + c_] = vr[it];
-    }
+  for (int it = 0; it < NIT; ++it) {
+    const int e = threadIdx.x + it * EPI_THREADS;
+    const int a_ = e / (EPI_C * EPI_B), c_ = (e / EPI_B) % EPI_C,
+              b_ = e % EPI_B;
+    const int a = a0 + a_, b = b0 + b_, c = c0 + c_;
+    const bool ok = a < v && b < a && c < b;
+    const int64_t off = ok ? (int64_t)c * ld + pairidx(a, b) : 0;
+    const int idx = (a_ * EPI_B + b_) * EPI_CS + c_;
+    cp_async8(&s3[idx], T + off, ok);
+    if (FT) cp_async8(&s3[S + idx], R + off, ok);
   }
-  __syncthreads();
 
   const int a_ = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int a = a0 + a_, c = c0 + lane;
@@ -143,40 +156,40 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
   const double f_ic = u2[i * v + cc], f_jc = u2[j * v + cc],
                f_kc = u2[k * v + cc];
   const double dia = p.d_a[i * v + ac], dkc = p.d_a[k * v + cc];
+  cp_async_wait_all();
+  __syncthreads();
 
-  double w_[EPI_B], r_[EPI_B], x_[EPI_B], d_[EPI_B];
-  bool ok_[EPI_B];
-#pragma unroll
-  for (int b_ = 0; b_ < EPI_B; ++b_) {
-    const int b = b0 + b_;
-    ok_[b_] = a < v && b < a && c < b;
-    const int bc = b < v ? b : v - 1;
-    const int cb = ok_[b_] ? c : 0;          // pair index needs c < b
-    const int64_t t1 = (int64_t)ac * ld + pairidx(bc, cb);
-    const int64_t t2 = (int64_t)bc * ld + pairidx(ac, cb);
-    const int is = (a_ * EPI_B + b_) * EPI_CS + lane;
-    w_[b_] = T[t1] - T[t2] + s3[is];
-    r_[b_] = FT ? R[t1] - R[t2] + s3[S + is] : 0.0;
-    const int64_t bc1 = (int64_t)bc * p.g1_ld_aa + cc,
-                  bc2 = (int64_t)bc * p.g2_ld_aa + cc;
-    const int64_t ba1 = (int64_t)bc * p.g1_ld_aa + ac,
-                  ba2 = (int64_t)bc * p.g2_ld_aa + ac;
-    // the 9-term sums of src/pt.c:166-174 for (t1, i_oovv) and (f_ov, t2)
-    x_[b_] = t1ia * g1jk[bc1] - t1ja * g1ik[bc1] - t1ka * g1ji[bc1] -
-             u1[i * v + bc] * A1jk + u1[j * v + bc] * A1ik +
-             u1[k * v + bc] * A1ji - t1ic * g1jk[ba1] + t1jc * g1ik[ba1] +
-             t1kc * g1ji[ba1] +
-             f_ia * g2jk[bc2] - f_ja * g2ik[bc2] - f_ka * g2ji[bc2] -
-             u2[i * v + bc] * A2jk + u2[j * v + bc] * A2ik +
-             u2[k * v + bc] * A2ji - f_ic * g2jk[ba2] + f_jc * g2ik[ba2] +
-             f_kc * g2ji[ba2];
-    d_[b_] = (dia + p.d_a[j * v + bc]) + dkc;
-  }
+  // one b at a time: the element's energy is added as soon as its operands
+  // are in (arrays of all 8 b values spilled registers); the loop is
+  // unrolled so the loads of later b overlap the arithmetic of earlier ones
   double e = 0.0;
 #pragma unroll
   for (int b_ = 0; b_ < EPI_B; ++b_) {
-    const double r = FT ? r_[b_] : w_[b_];
-    if (ok_[b_]) e += (w_[b_] - x_[b_]) * r / d_[b_];
+    const int b = b0 + b_;
+    const bool ok = a < v && b < a && c < b;
+    const int bc = b < v ? b : v - 1;
+    const int cb = ok ? c : 0;               // pair index needs c < b
+    const int t1 = ac * ldi + pair32(bc, cb);   // < 2^31 (plan check)
+    const int t2 = bc * ldi + pair32(ac, cb);
+    const int is = (a_ * EPI_B + b_) * EPI_CS + lane;
+    const double w = T[t1] - T[t2] + s3[is];
+    const double rr = FT ? R[t1] - R[t2] + s3[S + is] : w;
+    const int bc1 = bc * g1l + cc, bc2 = bc * g2l + cc;
+    const int ba1 = bc * g1l + ac, ba2 = bc * g2l + ac;
+    // the 9-term sums of src/pt.c:166-174 for (t1, i_oovv) and (f_ov, t2);
+    // the second is skipped when f_ov is zero (its terms would all be 0)
+    double x =
+        t1ia * g1jk[bc1] - t1ja * g1ik[bc1] - t1ka * g1ji[bc1] -
+        u1[i * v + bc] * A1jk + u1[j * v + bc] * A1ik +
+        u1[k * v + bc] * A1ji - t1ic * g1jk[ba1] + t1jc * g1ik[ba1] +
+        t1kc * g1ji[ba1];
+    if (has_f)
+      x += f_ia * g2jk[bc2] - f_ja * g2ik[bc2] - f_ka * g2ji[bc2] -
+           u2[i * v + bc] * A2jk + u2[j * v + bc] * A2ik +
+           u2[k * v + bc] * A2ji - f_ic * g2jk[ba2] + f_jc * g2ik[ba2] +
+           f_kc * g2ji[ba2];
+    const double dd = (dia + p.d_a[j * v + bc]) + dkc;
+    if (ok) e += (w - x) * rr / dd;
   }
   const double s = block_sum(e);
   if (threadIdx.x == 0) item.partials[local] = s;
@@ -216,15 +229,22 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
   const int i = item.i, j = item.j, k = item.k;
   const int oa = p.oa, va = p.va, ob = p.ob, vb = p.vb;
   const double *base = item.ws;
-  const int64_t ld1 = p.ld[0], ld2 = p.ld[1], ldp = p.ld[2];
-  const int64_t r1 = p.rowU1, r2 = p.rowU2;
+  const int64_t ld2 = p.ld[1], ldp = p.ld[2];
+  const int64_t r2 = p.rowU2;
+  // 32-bit strides for the per-element loop (the plan keeps a triple's
+  // arrays and the i_oovv / amplitude slices under 2^31 elements)
+  const int ld1 = (int)p.ld[0], r1 = (int)p.rowU1;
+  const int g1lab = (int)p.g1_ld_ab, g2lab = (int)p.g2_ld_ab;
+  const int g1laa = (int)p.g1_ld_aa, g2laa = (int)p.g2_ld_aa;
+  const bool has_f = p.has_f != 0;
 
+  // stage U2 (both orientations) and P asynchronously; the wait comes after
+  // the per-thread operand loads below
 #pragma unroll
   for (int side = 0; side < (FT ? 2 : 1); ++side) {
     const int64_t *off = side ? p.offR : p.offL;
     const double *U2 = base + off[1];
     const double *P = base + off[2];
-    double vx[NIT], vy[NIT], vp[NIT];
 #pragma unroll
     for (int it = 0; it < NIT; ++it) {
       const int e = threadIdx.x + it * EPI_THREADS;
@@ -232,27 +252,20 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
                 w = e % EPI_B;
       const int c = c0 + c_;
       const bool cok = c < vb;
-      const int ax = a0 + u, bx = b0 + w;     // x: U2[a][c][b]
-      vx[it] = (cok && ax < va && bx < va)
-                   ? U2[(int64_t)ax * ld2 + c * r2 + bx] : 0.0;
-      const int by = b0 + u, ay = a0 + w;     // y: U2[b][c][a]
-      vy[it] = (cok && ay < va && by < va)
-                   ? U2[(int64_t)by * ld2 + c * r2 + ay] : 0.0;
-      vp[it] = (cok && ax < va && bx < ax)    // p: P[c][pair(a,b)]
-                   ? P[(int64_t)c * ldp + pairidx(ax, bx)] : 0.0;
-    }
-#pragma unroll
-    for (int it = 0; it < NIT; ++it) {
-      const int e = threadIdx.x + it * EPI_THREADS;
-      const int u = e / (EPI_C * EPI_B), c_ = (e / EPI_B) % EPI_C,
-                w = e % EPI_B;
       const int idx = side * 3 * S + (u * EPI_B + w) * EPI_CS + c_;
-      sx[idx] = vx[it];
-      sy[idx] = vy[it];
-      sp[idx] = vp[it];
+      const int ax = a0 + u, bx = b0 + w;     // x: U2[a][c][b]
+      const bool okx = cok && ax < va && bx < va;
+      cp_async8(&sx[idx], U2 + (okx ? (int64_t)ax * ld2 + c * r2 + bx : 0),
+                okx);
+      const int by = b0 + u, ay = a0 + w;     // y: U2[b][c][a]
+      const bool oky = cok && ay < va && by < va;
+      cp_async8(&sy[idx], U2 + (oky ? (int64_t)by * ld2 + c * r2 + ay : 0),
+                oky);
+      const bool okp = cok && ax < va && bx < ax;   // p: P[c][pair(a,b)]
+      cp_async8(&sp[idx],
+                P + (okp ? (int64_t)c * ldp + pairidx(ax, bx) : 0), okp);
     }
   }
-  __syncthreads();
 
   const int a_ = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int a = a0 + a_, c = c0 + lane;
@@ -275,37 +288,33 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
   const double f_ia = u2[i * va + ac], f_ja = u2[j * va + ac];
   const double o1k = p.ov1_b[k * vb + cc], o2k = p.ov2_b[k * vb + cc];
   const double dia = p.d_a[i * va + ac], dkc = p.d_b[k * vb + cc];
+  cp_async_wait_all();
+  __syncthreads();
 
-  double w_[EPI_B], r_[EPI_B], x_[EPI_B], d_[EPI_B];
-  bool ok_[EPI_B];
-#pragma unroll
-  for (int b_ = 0; b_ < EPI_B; ++b_) {
-    const int b = b0 + b_;
-    ok_[b_] = a < va && b < a && c < vb;
-    const int bc = b < va ? b : va - 1;
-    const int64_t u_ab = (int64_t)ac * ld1 + bc * r1 + cc;
-    const int64_t u_ba = (int64_t)bc * ld1 + ac * r1 + cc;
-    const int ix = (a_ * EPI_B + b_) * EPI_CS + lane;
-    const int iy = (b_ * EPI_A + a_) * EPI_CS + lane;
-    w_[b_] = U1[u_ab] + sx[ix] - U1[u_ba] - sy[iy] + sp[ix];
-    r_[b_] = FT ? U1r[u_ab] + sx[3 * S + ix] - U1r[u_ba] - sy[3 * S + iy] +
-                      sp[3 * S + ix]
-                : 0.0;
-    const int64_t bc1 = (int64_t)bc * p.g1_ld_ab + cc,
-                  bc2 = (int64_t)bc * p.g2_ld_ab + cc;
-    x_[b_] = t1ia * g1jk[bc1] - u1[i * va + bc] * A1jk - t1ja * g1ik[bc1] +
-             u1[j * va + bc] * A1ik +
-             o1k * g1ji[(int64_t)bc * p.g1_ld_aa + ac] +
-             f_ia * g2jk[bc2] - u2[i * va + bc] * A2jk - f_ja * g2ik[bc2] +
-             u2[j * va + bc] * A2ik +
-             o2k * g2ji[(int64_t)bc * p.g2_ld_aa + ac];
-    d_[b_] = (dia + p.d_a[j * va + bc]) + dkc;
-  }
+  // one b at a time (see the same-spin kernel)
   double e = 0.0;
 #pragma unroll
   for (int b_ = 0; b_ < EPI_B; ++b_) {
-    const double r = FT ? r_[b_] : w_[b_];
-    if (ok_[b_]) e += (w_[b_] - x_[b_]) * r / d_[b_];
+    const int b = b0 + b_;
+    const bool ok = a < va && b < a && c < vb;
+    const int bc = b < va ? b : va - 1;
+    const int u_ab = ac * ld1 + bc * r1 + cc;   // < 2^31 (checked by
+    const int u_ba = bc * ld1 + ac * r1 + cc;   // the plan)
+    const int ix = (a_ * EPI_B + b_) * EPI_CS + lane;
+    const int iy = (b_ * EPI_A + a_) * EPI_CS + lane;
+    const double w = U1[u_ab] + sx[ix] - U1[u_ba] - sy[iy] + sp[ix];
+    const double rr = FT ? U1r[u_ab] + sx[3 * S + ix] - U1r[u_ba] -
+                               sy[3 * S + iy] + sp[3 * S + ix]
+                         : w;
+    const int bc1 = bc * g1lab + cc, bc2 = bc * g2lab + cc;
+    double x =
+        t1ia * g1jk[bc1] - u1[i * va + bc] * A1jk - t1ja * g1ik[bc1] +
+        u1[j * va + bc] * A1ik + o1k * g1ji[bc * g1laa + ac];
+    if (has_f)   // the (f_ov, t2) half, zero when f_ov is
+      x += f_ia * g2jk[bc2] - u2[i * va + bc] * A2jk - f_ja * g2ik[bc2] +
+           u2[j * va + bc] * A2ik + o2k * g2ji[bc * g2laa + ac];
+    const double dd = (dia + p.d_a[j * va + bc]) + dkc;
+    if (ok) e += (w - x) * rr / dd;
   }
   const double s = block_sum(e);
   if (threadIdx.x == 0) item.partials[local] = s;

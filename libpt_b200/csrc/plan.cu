@@ -617,6 +617,7 @@ int build_aaa(libpt_plan *p, SpinCase &c) {
   e.ntiles = c.ntiles;
   e.tiles = c.d_tiles;
   e.ctiles = c.ctiles;
+  e.has_f = p->has_f ? 1 : 0;
   const double vv = (double)v;
   c.flops_per_triple = 3.0 * vv * vv * vv * (vv - 1) + 6.0 * o * vv * vv * vv;
   if (p->ft) c.flops_per_triple *= 2;
@@ -746,6 +747,7 @@ int build_aab(libpt_plan *p, SpinCase &c) {
   e.ntiles = c.ntiles;
   e.tiles = c.d_tiles;
   e.ctiles = c.ctiles;
+  e.has_f = p->has_f ? 1 : 0;
   const double A = (double)va, B = (double)vb;
   c.flops_per_triple = 2 * A * A * A * B + 4 * A * A * B * B +
                        2 * B * A * A * (A - 1) + 6 * A * A * B * oa +
@@ -1469,6 +1471,16 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       r = LIBPT_ERR_CUDA;
       break;
     }
+    if (!g_dry) {   // an all-zero f_ov (the usual case) skips its terms
+      std::vector<double> f((size_t)nov);
+      if (cudaMemcpy(f.data(), p->ov2, (size_t)nov * 8,
+                     cudaMemcpyDeviceToHost) != cudaSuccess) {
+        r = LIBPT_ERR_CUDA;
+        break;
+      }
+      p->has_f = std::any_of(f.begin(), f.end(),
+                             [](double x) { return x != 0.0; });
+    }
     if ((r = add_cases(p))) break;
     if (p->precision != LIBPT_PREC_FP64) {
       // the tensor-core paths read planes; of the padded FP64 blocks only the
@@ -1512,6 +1524,12 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
         p->ntiles_max = std::max(p->ntiles_max, c.ntiles);
         p->jobs_max = std::max(p->jobs_max, c.jobs.size());
       }
+    if (p->ws_stride >= ((int64_t)1 << 31)) {
+      // the epilogue indexes a triple's outputs with 32-bit offsets
+      set_error("libpt_plan_create: orbital spaces too large (v > ~1000)");
+      r = LIBPT_ERR_ARG;
+      break;
+    }
     if ((r = upload_views(p))) break;
     if (p->queue.empty()) break;
     if (p->arena) {

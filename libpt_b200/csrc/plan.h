@@ -119,6 +119,7 @@ struct libpt_plan {
   std::vector<void *> allocs;
   ptb::OperandSet L, R;
   double *d_ov = nullptr, *ov1 = nullptr, *ov2 = nullptr;
+  bool has_f = true;                    // f_ov / f2_ov not all zero
   double *oovv[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<ptb::SpinCase> cases;
   std::vector<int4> queue;              // (case, i, j, k)
