@@ -84,6 +84,15 @@ def parse():
 
 PRECISIONS = {"fp64": 0, "tf32x3": 1, "emu64": 2}
 
+# DRAM bytes (read + write) per reference flop of the contraction kernels,
+# from one ncu capture each of restricted (T) o=2, v=477 (two mixed-spin
+# triples, 9.26e11 flops; profiles/gemm_dmma_rpt_o2_v477_fp64_full.txt and
+# profiles/gemm_i8_rpt_o2_v477_emu64s6_full.txt).  A launch's traffic grows
+# with its triples (each reads its own operand slices and writes its own
+# outputs), so the bench scales these by the flops of its launches.
+DRAM_BYTES_PER_FLOP = {"gemm_dmma_kernel": (7.141e9 + 4.338e9) / 9.26e11,
+                       "gemm_i8_kernel": (11.894e9 + 4.337e9) / 9.26e11}
+
 
 # ------------------------------------------------------------------ helpers
 
@@ -429,7 +438,11 @@ def run_ours(args, d):
                 flops_per_step=flops_step),
             projected_solve_seconds=flops_full / (value / d.world * 1e12),
             roofline=dict(bound="tensor", achieved=ach, peak=peak64,
-                          unit="TFLOP/s", frac=ach / peak64, traffic=None,
+                          unit="TFLOP/s", frac=ach / peak64,
+                          traffic=DRAM_BYTES_PER_FLOP["gemm_dmma_kernel"] *
+                          stats["gemm_flops"] / max(stats["gemm_launches"], 1),
+                          traffic_note="bytes per launch, scaled from the "
+                                       "o=2 v=477 ncu capture by flops",
                           kernel="gemm_dmma_kernel",
                           peak_source="cuBLAS DGEMM n=8192 burst, measured "
                                       "in this run (FP64 tensor)",
@@ -448,7 +461,13 @@ def run_ours(args, d):
                 ratio_to_head=Rr["value"] / value,
                 ms_per_step=Rr["secs_max"] / args.steps * 1e3,
                 projected_solve_seconds=Rr["flops_full"] / (Rr["value"] / d.world * 1e12),
-                gemm_tflops=Rr["gemm"], energy_sample=Rr["energy"],
+                gemm_tflops=Rr["gemm"],
+                gemm_traffic_per_launch=(
+                    DRAM_BYTES_PER_FLOP["gemm_i8_kernel"] *
+                    Rr["stats"]["gemm_flops"] /
+                    max(Rr["stats"]["gemm_launches"], 1))
+                if name == "emu64" else None,
+                energy_sample=Rr["energy"],
                 energy_sample_delta=Rr["energy"] - energy_sample,
                 slices=args.slices if name == "emu64" else None,
                 epilogue_ms_share=Rr["stats"]["epi_ms"] / max(Rr["secs"] * 1e3, 1e-9),
