@@ -18,6 +18,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "plan.h"
@@ -318,15 +320,67 @@ int dalloc(libpt_plan *p, void **ptr, size_t bytes) {
   return LIBPT_OK;
 }
 
+// Page-locked staging for host uploads, shared by the process: two 64 MiB
+// buffers used in turn, so the host copy of one chunk into page-locked
+// memory overlaps the DMA of the previous one (pageable cudaMemcpyAsync
+// copies through the driver's own small buffers, synchronously).
+struct PinnedRing {
+  std::mutex mu;   // one upload uses the ring at a time
+  char *buf[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  bool tried = false, ok = false;
+  static constexpr size_t BYTES = (size_t)64 << 20;
+  bool ready() {   // with mu held
+    if (tried) return ok;
+    tried = true;
+    ok = true;
+    for (int b = 0; b < 2 && ok; ++b)
+      ok = cudaHostAlloc((void **)&buf[b], BYTES, cudaHostAllocDefault) ==
+               cudaSuccess &&
+           cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming) ==
+               cudaSuccess;
+    if (!ok) cudaGetLastError();
+    return ok;
+  }
+};
+
+PinnedRing &pinned_ring() {
+  static PinnedRing r;
+  return r;
+}
+
+// memcpy with up to 8 host threads (large chunks only).
+void par_memcpy(void *dst, const void *src, size_t n) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned T = std::min(8u, hw);
+  if (n < ((size_t)8 << 20) || T < 2) {
+    std::memcpy(dst, src, n);
+    return;
+  }
+  const size_t per = (n / T + 4095) & ~(size_t)4095;
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < T; ++t) {
+    const size_t o = t * per;
+    if (o >= n) break;
+    th.emplace_back([=] {
+      std::memcpy((char *)dst + o, (const char *)src + o, std::min(per, n - o));
+    });
+  }
+  std::memcpy(dst, src, std::min(per, n));
+  for (auto &x : th) x.join();
+}
+
 // Copies rows x w elements (FP64 or FP32, host or device) into a padded FP64
-// device block rows x dpitch.  Host sources go through a device staging
-// buffer in chunks.
+// device block rows x dpitch.  Host sources go through page-locked and
+// device staging buffers in chunks of whole rows (two of each, used in
+// turn), device sources are repacked directly.
 struct Uploader {
   libpt_plan *p;
   bool host, fp32;
-  size_t stage_cap = (size_t)256 << 20;   // staging buffer bound
-  void *stage = nullptr;
+  size_t stage_cap = PinnedRing::BYTES;   // per staging buffer
+  void *stage[2] = {nullptr, nullptr};    // device staging
   size_t stage_bytes = 0;
+  int slot = 0;
 
   int put(double *dst, const void *src, int64_t rows, int64_t w,
           int64_t dpitch) {
@@ -335,33 +389,49 @@ struct Uploader {
     if (!host) {
       if (w == dpitch && !fp32)
         DEV(cudaMemcpyAsync(dst, src, (size_t)rows * w * 8,
-                           cudaMemcpyDeviceToDevice, p->st));
+                            cudaMemcpyDeviceToDevice, p->st));
       else
         DEV(repack_launch(src, fp32, dst, rows, w, dpitch, p->st));
       return LIBPT_OK;
     }
-    if (!stage) {
+    if (!stage[0]) {
       stage_bytes = stage_cap;
-      if (dalloc(p, &stage, stage_bytes)) return LIBPT_ERR_NOMEM;
+      if (dalloc(p, &stage[0], stage_bytes) || dalloc(p, &stage[1], stage_bytes))
+        return LIBPT_ERR_NOMEM;
     }
-    if (w == dpitch) {   // unpadded: copy as a flat array
-      const int64_t total = rows * w, chunk = (int64_t)(stage_bytes / es);
-      for (int64_t x0 = 0; x0 < total; x0 += chunk) {
-        const int64_t nx = std::min(chunk, total - x0);
-        DEV(cudaMemcpyAsync(stage, (const char *)src + (size_t)x0 * es,
-                           (size_t)nx * es, cudaMemcpyHostToDevice, p->st));
-        DEV(repack_launch(stage, fp32, dst + x0, 1, nx, nx, p->st));
-      }
-      return LIBPT_OK;
-    }
+    if (g_dry) return LIBPT_OK;
+    // chunks: whole rows (a flat run of elements when unpadded)
+    const bool flat = w == dpitch;
+    const int64_t unit = flat ? 1 : std::max<int64_t>(w, 1);
+    const int64_t total = flat ? rows * w : rows;
     const int64_t chunk =
-        std::max<int64_t>(1, (int64_t)(stage_bytes / (es * std::max<int64_t>(w, 1))));
-    for (int64_t r0 = 0; r0 < rows; r0 += chunk) {
-      const int64_t nr = std::min(chunk, rows - r0);
-      DEV(cudaMemcpyAsync(stage, (const char *)src + (size_t)r0 * w * es,
-                         (size_t)nr * w * es, cudaMemcpyHostToDevice, p->st));
-      DEV(repack_launch(stage, fp32, dst + r0 * dpitch, nr, w, dpitch, p->st));
+        std::max<int64_t>(1, (int64_t)(stage_bytes / (es * unit)));
+    PinnedRing &ring = pinned_ring();
+    std::lock_guard<std::mutex> lk(ring.mu);
+    const bool pinned = ring.ready();
+    for (int64_t x0 = 0; x0 < total; x0 += chunk) {
+      const int64_t nx = std::min(chunk, total - x0);
+      const size_t bytes = (size_t)(nx * unit) * es;
+      const char *from = (const char *)src + (size_t)(x0 * unit) * es;
+      void *dstage = stage[slot];
+      if (pinned) {
+        CK(cudaEventSynchronize(ring.done[slot]));   // its last DMA is done
+        par_memcpy(ring.buf[slot], from, bytes);
+        CK(cudaMemcpyAsync(dstage, ring.buf[slot], bytes,
+                           cudaMemcpyHostToDevice, p->st));
+        CK(cudaEventRecord(ring.done[slot], p->st));
+      } else {
+        CK(cudaMemcpyAsync(dstage, from, bytes, cudaMemcpyHostToDevice, p->st));
+      }
+      if (flat)
+        CK(repack_launch(dstage, fp32, dst + x0, 1, nx, nx, p->st));
+      else
+        CK(repack_launch(dstage, fp32, dst + x0 * dpitch, nx, w, dpitch,
+                         p->st));
+      slot ^= 1;
     }
+    // the ring's buffers may be reused by the next upload only after these
+    // DMAs: each slot's event covers its last copy
     return LIBPT_OK;
   }
 };
@@ -1424,7 +1494,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     Sizes S{(int64_t)oa, (int64_t)va, (int64_t)ob, (int64_t)vb};
     Uploader up{p, host, dtype == 1};
     {
-      // staging: no larger than the largest argument array (256 MiB at most)
+      // staging: no larger than the largest argument array (64 MiB at most)
       int64_t big = (int64_t)(oa * va + (unr ? ob * vb : 0));
       int64_t t2 = 0, oo = 0, vv = 0;
       for (int b = 0; b < (unr ? 4 : 2); ++b) {
@@ -1435,6 +1505,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       big = std::max({big, t2, oo, vv});
       const size_t bytes = (size_t)big * (dtype ? 4 : 8);
       up.stage_cap = std::max<size_t>(256, std::min(up.stage_cap, (bytes + 255) & ~size_t(255)));
+      // (two device staging buffers of this size; see Uploader)
     }
     const int64_t nov = (int64_t)(oa * va + (unr ? ob * vb : 0));
     if ((r = dalloc(p, (void **)&p->d_ov, nov * 8 + 8))) break;
