@@ -26,9 +26,12 @@ Lines printed (rank 0, one JSON line):
 --impl reference prints the reference's own CPU implementation on the same
 sample workload (o=2, v=477 full solves), with all host threads.
 
-Multi-GPU (torchrun): every rank solves its own replica (replicas only; the
-path's triples shard with no data exchange, but one GPU per solve is the
-design), scaling "weak", time = max over ranks.
+Multi-GPU (torchrun): the ranks shard one solve the way the reference's MPI
+build does (src/pt.c:213, 474-477): identical inputs on every GPU, a sample
+N times denser whose entry q runs on rank q % N, and per step one sum
+all-reduce of the per-triple energy slots (NCCL); scaling "weak" (fixed
+triples per GPU), time = max over ranks.  The e2e figure stays one host-API
+solve per rank.
 """
 import argparse
 import csv
@@ -311,8 +314,8 @@ def run_ours(args, d):
 
     # ---- operands: generated on the device, then planned (resident) -------
     t_gen = time.perf_counter()
-    meta, tens = synth.rpt_case_device(args.o, args.v, seed=1000 + d.rank,
-                                       device=dev)
+    # the same inputs on every rank (a sharded solve needs identical copies)
+    meta, tens = synth.rpt_case_device(args.o, args.v, seed=1000, device=dev)
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t_gen
     naaa = args.o * (args.o - 1) * (args.o - 2) // 6
@@ -328,11 +331,28 @@ def run_ours(args, d):
         del src
         torch.cuda.synchronize()
         t_plan = time.perf_counter() - t0
-        sample = np.arange(0, plan.n, args.stride, dtype=np.int64)
+        # N ranks: a sample N times denser, entry q of it on rank q % N
+        gsample = np.arange(0, plan.n, max(1, args.stride // d.world),
+                            dtype=np.int64)
+        sample = gsample[d.rank::d.world]
         flops_step = sum(plan.flops(int(q), 1) for q in sample)
+        flops_all = d.sum(flops_step)
         flops_full = plan.flops()
-        for _ in range(args.warmup):
+        slots = exch = None
+        if d.world > 1:
+            # the ranks' energies meet in one slot all-reduce per step; the
+            # plan's own slots keep only this rank's entries
+            slots = plan.energy_slots()
+            exch = torch.empty_like(slots)
+
+        def step():
             plan.run(sample)
+            if exch is not None:
+                exch.copy_(slots)
+                d.pg.all_reduce(exch)
+
+        for _ in range(args.warmup):
+            step()
             plan.energy(sample)
         plan.timing(True)
         plan.kernel_stats()
@@ -343,7 +363,7 @@ def run_ours(args, d):
         s_ev, e_ev = torch.cuda.Event(True), torch.cuda.Event(True)
         s_ev.record()
         for _ in range(args.steps):
-            plan.run(sample)
+            step()
         e_ev.record()
         torch.cuda.synchronize()
         d.barrier()
@@ -351,14 +371,20 @@ def run_ours(args, d):
         secs = s_ev.elapsed_time(e_ev) / 1e3
         secs_max = d.max(secs)
         stats = plan.kernel_stats()
-        energy = plan.energy(sample)
+        if exch is not None:    # the whole sample's energy, from the exchange
+            energy = 2.0 * ffi.energy_sum(exch.cpu().numpy()[gsample])
+            del slots
+        else:
+            energy = plan.energy(sample)
         n = plan.n
         plan.close()
         torch.cuda.empty_cache()
         return dict(sample=sample, flops_step=flops_step, flops_full=flops_full,
                     secs=secs, secs_max=secs_max, stats=stats, clk=clk,
                     energy=energy, n=n, plan_seconds=t_plan,
-                    value=d.world * args.steps * flops_step / secs_max / 1e12,
+                    flops_all=flops_all, nsample=len(gsample),
+                    nsame=int((gsample < naaa).sum()),
+                    value=args.steps * flops_all / secs_max / 1e12,
                     gemm=stats["gemm_flops"] / (stats["gemm_ms"] / 1e3) / 1e12)
 
     runs = {}
@@ -429,14 +455,17 @@ def run_ours(args, d):
             higher_is_better=True, scaling="weak", vs_baseline=None,
             dtype="f64", data="synthetic",
             config=dict(
-                workload=f"rpt o={args.o} v={args.v}: every {args.stride}th "
-                         f"triple of the {plan_n}-entry queue per step "
-                         f"({len(sample)} triples, "
-                         f"{int((sample < naaa).sum())} same-spin)",
-                precision=head, parallelism=f"replicas x{d.world}",
+                workload=f"rpt o={args.o} v={args.v}: every "
+                         f"{max(1, args.stride // d.world)}th triple of the "
+                         f"{plan_n}-entry queue per step ({R0['nsample']} "
+                         f"triples, {R0['nsame']} same-spin)",
+                precision=head,
+                parallelism="1 GPU" if d.world == 1 else
+                f"triples sharded x{d.world} (entry q on rank q % "
+                f"{d.world}), one energy-slot all-reduce per step",
                 l2="inputs (74 GB) larger than L2; no flush needed",
-                flops_per_step=flops_step),
-            projected_solve_seconds=flops_full / (value / d.world * 1e12),
+                flops_per_step=R0["flops_all"]),
+            projected_solve_seconds=flops_full / (value * 1e12),
             roofline=dict(bound="tensor", achieved=ach, peak=peak64,
                           unit="TFLOP/s", frac=ach / peak64,
                           traffic=DRAM_BYTES_PER_FLOP["gemm_dmma_kernel"] *
@@ -460,7 +489,7 @@ def run_ours(args, d):
                 value=Rr["value"], unit="TFLOP/s",
                 ratio_to_head=Rr["value"] / value,
                 ms_per_step=Rr["secs_max"] / args.steps * 1e3,
-                projected_solve_seconds=Rr["flops_full"] / (Rr["value"] / d.world * 1e12),
+                projected_solve_seconds=Rr["flops_full"] / (Rr["value"] * 1e12),
                 gemm_tflops=Rr["gemm"],
                 gemm_traffic_per_launch=(
                     DRAM_BYTES_PER_FLOP["gemm_i8_kernel"] *

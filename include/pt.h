@@ -115,7 +115,11 @@ const char *libpt_last_error(void);
                                  smallest S whose error bound, estimated on a
                                  sample of triples against 7 slices, is under
                                  LIBPT_EMU_TOL / 2 (environment, Eh; default
-                                 1e-6, the north star's 1 uEh)               */
+                                 1e-6, i.e. 1 uEh).  The FP64 entry points
+                                 (libpt_rpt ... and their _dev twins) use it
+                                 when the environment sets
+                                 LIBPT_FP64_PRECISION=emu64 (S chosen) or
+                                 emu64:S; otherwise they run FP64 DMMA      */
 
 /* Built-in self-test of a contraction kernel: C = A B1 - A B2 on random
  * m x k and k x n operands, against an FP64 reference computed on the device;
@@ -247,6 +251,36 @@ int libpt_plan_run_all(libpt_plan *plan);
 int libpt_plan_energy(libpt_plan *plan, const int64_t *idx, size_t n,
     double *e_out);
 int libpt_plan_destroy(libpt_plan *plan);
+
+/* ---- one solve sharded over ranks (src/pt.c:197-221, 474-477) ----------
+ *
+ * The reference's MPI scheme on GPUs: every rank (one per GPU) creates a
+ * plan from the same inputs and runs the queue entries it owns, entry q
+ * belonging to rank q % size (src/pt.c:213, `it % size == rank`).  The
+ * ranks then add their per-triple energy slots -- queue_length doubles on
+ * the device, zero where another rank owns the entry -- with one in-place
+ * sum all-reduce (ncclAllReduce, or MPI_Allreduce on a host copy), the
+ * counterpart of the reference's one-double MPI_Allreduce (src/pt.c:
+ * 474-477).  libpt_plan_energy on any rank then returns the one-GPU energy
+ * bitwise: each slot holds exactly its owner's value, and the sum runs in
+ * queue order as for an unsharded solve. */
+
+/* Writes to idx (when non-NULL) the queue entries rank `rank` of `size`
+ * owns, in increasing order; returns their number, -1 for invalid
+ * arguments.  Host-only: needs no device. */
+int64_t libpt_shard_entries(int64_t queue_length, int rank, int size,
+    int64_t *idx);
+/* Zeroes all of the plan's energy slots, then runs the entries rank `rank`
+ * of `size` owns.  Asynchronous on the plan's stream. */
+int libpt_plan_run_shard(libpt_plan *plan, int rank, int size);
+/* Device address of the plan's per-triple energies (queue_length doubles,
+ * queue order, restricted factor not applied).  Valid until the plan is
+ * destroyed; the caller may overwrite it (e.g. with an all-reduce) once the
+ * plan's stream has finished its runs. */
+int libpt_plan_energy_slots(libpt_plan *plan, double **slots);
+/* Host-only: the queue-order compensated sum libpt_plan_energy applies
+ * (without the restricted factor 2) of energies[0..n). */
+int libpt_energy_sum(const double *energies, size_t n, double *e_out);
 
 /* Kernel timing for benchmarks: with timing enabled, each batch records CUDA
  * events around its contraction (GEMM) and energy (epilogue) launches on the

@@ -25,6 +25,18 @@ int mp_precision() {
   return LIBPT_PREC_FP64;
 }
 
+// Precision of the FP64 entry points: the FP64 engine, or emulated FP64
+// when LIBPT_FP64_PRECISION=emu64 (digit slices chosen per solve for the
+// LIBPT_EMU_TOL tolerance, default 1e-6 Eh) or emu64:S (S = 4..7 fixed).
+int fp64_precision() {
+  const char *e = getenv("LIBPT_FP64_PRECISION");
+  if (!e || (e[0] != 'e' && e[0] != 'E')) return LIBPT_PREC_FP64;
+  const char *c = e;
+  while (*c && *c != ':') ++c;
+  const int s = *c ? atoi(c + 1) : 0;
+  return LIBPT_PREC_EMU64 | ((s >= 4 && s <= 7 ? s : 0) << 8);
+}
+
 [[noreturn]] void fatal(const char *where) {
   fprintf(stderr, "libpt: %s: %s\n", where, ptb::last_error());
   abort();
@@ -43,7 +55,7 @@ double host_solve(const char *name, int kind, size_t oa, size_t va, size_t ob,
   libpt_plan *p = nullptr;
   double e = 0.0;
   int r = ptb::plan_create(kind, oa, va, ob, vb, args, dtype,
-                           dtype ? mp_precision() : LIBPT_PREC_FP64, true, st,
+                           dtype ? mp_precision() : fp64_precision(), true, st,
                            &p);
   if (!r) r = ptb::plan_run(p, nullptr, p->queue.size());
   if (!r) r = ptb::plan_energy(p, nullptr, 0, &e);
@@ -62,7 +74,7 @@ int dev_solve(int kind, size_t oa, size_t va, size_t ob, size_t vb,
   }
   libpt_plan *p = nullptr;
   int r = ptb::plan_create(kind, oa, va, ob, vb, args, dtype,
-                           dtype ? mp_precision() : LIBPT_PREC_FP64, false,
+                           dtype ? mp_precision() : fp64_precision(), false,
                            static_cast<cudaStream_t>(stream), &p);
   if (!r) r = ptb::plan_run(p, nullptr, p->queue.size());
   if (!r) r = ptb::plan_energy(p, nullptr, 0, e_out);
@@ -306,6 +318,41 @@ LIBPT_API int libpt_plan_energy(libpt_plan *plan, const int64_t *idx,
     return LIBPT_ERR_ARG;
   }
   return ptb::plan_energy(plan, idx, n, e_out);
+}
+
+// ---- a solve sharded over ranks (src/pt.c:197-221, 474-477) ---------------
+
+LIBPT_API int64_t libpt_shard_entries(int64_t queue_length, int rank, int size,
+                                      int64_t *idx) {
+  const int64_t n = ptb::shard_entries(queue_length, rank, size, idx);
+  if (n < 0) ptb::set_error("libpt_shard_entries: invalid rank or size");
+  return n;
+}
+
+LIBPT_API int libpt_plan_run_shard(libpt_plan *plan, int rank, int size) {
+  if (!plan) {
+    ptb::set_error("libpt_plan_run_shard: NULL plan");
+    return LIBPT_ERR_ARG;
+  }
+  return ptb::plan_run_shard(plan, rank, size);
+}
+
+LIBPT_API int libpt_plan_energy_slots(libpt_plan *plan, double **slots) {
+  if (!plan || !slots) {
+    ptb::set_error("libpt_plan_energy_slots: NULL argument");
+    return LIBPT_ERR_ARG;
+  }
+  *slots = plan->e_slot;
+  return LIBPT_OK;
+}
+
+LIBPT_API int libpt_energy_sum(const double *energies, size_t n,
+                               double *e_out) {
+  if ((!energies && n) || !e_out) {
+    ptb::set_error("libpt_energy_sum: NULL argument");
+    return LIBPT_ERR_ARG;
+  }
+  return ptb::sum_slots(energies, n, nullptr, 0, e_out);
 }
 
 LIBPT_API int libpt_plan_timing(libpt_plan *plan, int enable) {

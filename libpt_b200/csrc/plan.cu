@@ -1751,13 +1751,21 @@ int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e,
     set_error("a device-side wait exceeded its time limit");
     return LIBPT_ERR_TIMEOUT;
   }
+  double s = 0.0;
+  if (int r = sum_slots(slots, total, idx, n, &s)) return r;
+  *e = p->factor * s;
+  return LIBPT_OK;
+}
+
+int sum_slots(const double *slots, size_t total, const int64_t *idx, size_t n,
+              double *out) {
   // Neumaier-compensated sum in queue order
   double s = 0.0, comp = 0.0;
   const size_t m = idx ? n : total;
   for (size_t x = 0; x < m; ++x) {
     const int64_t q = idx ? idx[x] : (int64_t)x;
     if (q < 0 || (size_t)q >= total) {
-      set_error("libpt_plan_energy: queue index out of range");
+      set_error("energy sum: queue index out of range");
       return LIBPT_ERR_ARG;
     }
     const double v = slots[q];
@@ -1765,8 +1773,34 @@ int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e,
     comp += std::fabs(s) >= std::fabs(v) ? (s - t) + v : (v - t) + s;
     s = t;
   }
-  *e = p->factor * (s + comp);
+  *out = s + comp;
   return LIBPT_OK;
+}
+
+int64_t shard_entries(int64_t total, int rank, int size, int64_t *idx) {
+  // src/pt.c:213: triple `it` belongs to rank it % size
+  if (total < 0 || size < 1 || rank < 0 || rank >= size) return -1;
+  int64_t n = 0;
+  for (int64_t q = rank; q < total; q += size) {
+    if (idx) idx[n] = q;
+    ++n;
+  }
+  return n;
+}
+
+int plan_run_shard(libpt_plan *p, int rank, int size) {
+  const int64_t total = (int64_t)p->queue.size();
+  const int64_t n = shard_entries(total, rank, size, nullptr);
+  if (n < 0) {
+    set_error("libpt_plan_run_shard: rank outside [0, size)");
+    return LIBPT_ERR_ARG;
+  }
+  // every slot this rank does not own stays zero, so that summing the ranks'
+  // slot arrays leaves each triple's energy exactly as its owner computed it
+  CK(cudaMemsetAsync(p->e_slot, 0, (total + 1) * 8, p->st));
+  std::vector<int64_t> ents((size_t)n);
+  shard_entries(total, rank, size, ents.data());
+  return run_entries(p, ents);
 }
 
 }  // namespace ptb

@@ -214,6 +214,15 @@ GemmGroup plan_group(const libpt_plan *p, const SpinCase &c);
 // sums them in queue order (restricted factor applied).
 int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e,
                 cudaStream_t rs = nullptr);
+// Queue-order compensated sum of slots[idx[0..n)] (idx NULL: all `total`),
+// without the restricted factor; the sum libpt_plan_energy applies.
+int sum_slots(const double *slots, size_t total, const int64_t *idx, size_t n,
+              double *out);
+// Entries of queue length `total` that rank `rank` of `size` owns (q % size
+// == rank); writes them to idx when non-NULL; -1 for invalid arguments.
+int64_t shard_entries(int64_t total, int rank, int size, int64_t *idx);
+// Zeroes every energy slot, then runs the entries rank `rank` owns.
+int plan_run_shard(libpt_plan *p, int rank, int size);
 void plan_destroy(libpt_plan *p);
 double plan_flops(const libpt_plan *p, int64_t first, int64_t n);
 int plan_kernel_stats(libpt_plan *p, double *gemm_ms, int64_t *gemm_launches,

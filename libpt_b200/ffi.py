@@ -115,6 +115,16 @@ def lib():
     L.libpt_server_destroy.argtypes = [vp]
     L.libpt_plan_destroy.restype = ctypes.c_int
     L.libpt_plan_destroy.argtypes = [vp]
+    L.libpt_shard_entries.restype = ctypes.c_int64
+    L.libpt_shard_entries.argtypes = [ctypes.c_int64, ctypes.c_int,
+                                      ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int64)]
+    L.libpt_plan_run_shard.restype = ctypes.c_int
+    L.libpt_plan_run_shard.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.libpt_plan_energy_slots.restype = ctypes.c_int
+    L.libpt_plan_energy_slots.argtypes = [vp, ctypes.POINTER(vp)]
+    L.libpt_energy_sum.restype = ctypes.c_int
+    L.libpt_energy_sum.argtypes = [dp, sz, dp]
     _lib = L
     return L
 
@@ -275,6 +285,36 @@ class Server:
             pass
 
 
+def shard_entries(queue_length, rank, size):
+    """Queue entries rank `rank` of `size` owns (q % size == rank)."""
+    n = lib().libpt_shard_entries(queue_length, rank, size, None)
+    if n < 0:
+        raise LibptError(1, lib().libpt_last_error().decode())
+    a = np.empty(n, dtype=np.int64)
+    lib().libpt_shard_entries(queue_length, rank, size,
+                              a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    return a
+
+
+def energy_sum(energies):
+    """The library's queue-order compensated sum of per-triple energies."""
+    a = np.ascontiguousarray(energies, dtype=np.float64)
+    e = ctypes.c_double()
+    check(lib().libpt_energy_sum(
+        a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), a.size,
+        ctypes.byref(e)))
+    return e.value
+
+
+class _DeviceArray:
+    """float64 device memory owned by the library, exposed to torch."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {
+            "shape": (n,), "typestr": "<f8", "data": (ptr, False),
+            "version": 3, "strides": None}
+
+
 class Plan:
     """Resident operands of one solve and its triples queue (libpt_plan_*)."""
 
@@ -316,6 +356,18 @@ class Plan:
                 self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
                 a.size, ctypes.byref(e)))
         return e.value
+
+    def run_shard(self, rank, size):
+        """Zero the energy slots, run the entries rank `rank` of `size` owns."""
+        check(lib().libpt_plan_run_shard(self.h, rank, size))
+
+    def energy_slots(self):
+        """The plan's per-triple energies as a CUDA float64 tensor (a view of
+        the plan's own device memory, valid while the plan lives)."""
+        import torch
+        ptr = ctypes.c_void_p()
+        check(lib().libpt_plan_energy_slots(self.h, ctypes.byref(ptr)))
+        return torch.as_tensor(_DeviceArray(ptr.value, self.n), device="cuda")
 
     def timing(self, enable=True):
         check(lib().libpt_plan_timing(self.h, 1 if enable else 0))
