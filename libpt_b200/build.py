@@ -16,6 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libpt_b200.so")
+CLI = os.path.join(LIBDIR, "pt_benchmark")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -60,6 +61,15 @@ def build(force=False, verbose=False):
         cmd = [NVCC, "-ccbin", HOST_CXX] + ARCH + ["-shared", "-o", LIB] + objs
         cmd += ["-Xcompiler", "-fPIC", "-lcudart_static", "-ldl", "-lrt",
                 "-lpthread"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    # the reference's benchmark command line against this library
+    cli_src = os.path.join(HERE, "cli", "pt_benchmark.c")
+    if force or _newer(CLI, [cli_src, LIB, os.path.join(ROOT, "include", "pt.h")]):
+        cmd = ["/usr/bin/gcc", "-O2", "-std=c11", "-Wall",
+               "-I" + os.path.join(ROOT, "include"), cli_src, "-o", CLI,
+               "-L" + LIBDIR, "-lpt_b200", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
