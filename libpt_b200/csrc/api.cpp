@@ -54,11 +54,19 @@ double host_solve(const char *name, int kind, size_t oa, size_t va, size_t ob,
   }
   libpt_plan *p = nullptr;
   double e = 0.0;
+  const double t0 = ptb::wall_seconds();
   int r = ptb::plan_create(kind, oa, va, ob, vb, args, dtype,
                            dtype ? mp_precision() : fp64_precision(), true, st,
                            &p);
+  const double t1 = ptb::wall_seconds();
   if (!r) r = ptb::plan_run(p, nullptr, p->queue.size());
   if (!r) r = ptb::plan_energy(p, nullptr, 0, &e);
+  if (!r && ptb::profile_enabled())
+    fprintf(stderr,
+            "libpt: %s oa=%zu va=%zu ob=%zu vb=%zu: upload %.3f s, prepare "
+            "%.3f s, tune %.3f s, create %.3f s, triples %.3f s\n",
+            name, oa, va, ob, vb, p->prof_upload, p->prof_prepare,
+            p->prof_tune, t1 - t0, ptb::wall_seconds() - t1);
   ptb::plan_destroy(p);
   cudaStreamDestroy(st);
   if (r) fatal(name);

@@ -14,9 +14,11 @@
 // slots indexed by queue position and are summed in queue order.
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <ctime>
 #include <string>
 #include <mutex>
 #include <thread>
@@ -349,25 +351,80 @@ PinnedRing &pinned_ring() {
   return r;
 }
 
-// memcpy with up to 8 host threads (large chunks only).
+// Host copies with up to 8 threads (large chunks only): a pool of worker
+// threads started on first use and kept for the life of the process (it is
+// never destroyed, so no worker outlives its state at exit).
+class CopyPool {
+ public:
+  static CopyPool &get() {
+    static CopyPool *pool = new CopyPool();
+    return *pool;
+  }
+
+  void copy(void *dst, const void *src, size_t n) {
+    if (n < ((size_t)8 << 20) || nw_ == 0) {
+      std::memcpy(dst, src, n);
+      return;
+    }
+    std::lock_guard<std::mutex> one_at_a_time(submit_mu_);
+    const size_t per = (n / (nw_ + 1) + 4095) & ~(size_t)4095;
+    {
+      std::lock_guard<std::mutex> g(mu_);
+      dst_ = static_cast<char *>(dst);
+      src_ = static_cast<const char *>(src);
+      n_ = n;
+      per_ = per;
+      pending_ = nw_;
+      ++gen_;
+    }
+    work_cv_.notify_all();
+    std::memcpy(dst, src, std::min(per, n));   // part 0 on this thread
+    std::unique_lock<std::mutex> g(mu_);
+    done_cv_.wait(g, [&] { return pending_ == 0; });
+  }
+
+ private:
+  CopyPool() {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned want = std::min(8u, hw) - 1;
+    for (unsigned t = 1; t <= want; ++t) {
+      try {
+        std::thread([this, t] { work(t); }).detach();
+        nw_ = t;
+      } catch (...) {
+        break;
+      }
+    }
+  }
+
+  void work(unsigned t) {
+    uint64_t seen = 0;
+    for (;;) {
+      std::unique_lock<std::mutex> g(mu_);
+      work_cv_.wait(g, [&] { return gen_ != seen; });
+      seen = gen_;
+      char *d = dst_;
+      const char *s = src_;
+      const size_t n = n_, o = (size_t)t * per_, len = per_;
+      g.unlock();
+      if (o < n) std::memcpy(d + o, s + o, std::min(len, n - o));
+      g.lock();
+      if (--pending_ == 0) done_cv_.notify_one();
+    }
+  }
+
+  unsigned nw_ = 0;   // workers; part t of a copy goes to worker t
+  std::mutex submit_mu_, mu_;
+  std::condition_variable work_cv_, done_cv_;
+  uint64_t gen_ = 0;
+  unsigned pending_ = 0;
+  char *dst_ = nullptr;
+  const char *src_ = nullptr;
+  size_t n_ = 0, per_ = 0;
+};
+
 void par_memcpy(void *dst, const void *src, size_t n) {
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const unsigned T = std::min(8u, hw);
-  if (n < ((size_t)8 << 20) || T < 2) {
-    std::memcpy(dst, src, n);
-    return;
-  }
-  const size_t per = (n / T + 4095) & ~(size_t)4095;
-  std::vector<std::thread> th;
-  for (unsigned t = 1; t < T; ++t) {
-    const size_t o = t * per;
-    if (o >= n) break;
-    th.emplace_back([=] {
-      std::memcpy((char *)dst + o, (const char *)src + o, std::min(per, n - o));
-    });
-  }
-  std::memcpy(dst, src, std::min(per, n));
-  for (auto &x : th) x.join();
+  CopyPool::get().copy(dst, src, n);
 }
 
 // Copies rows x w elements (FP64 or FP32, host or device) into a padded FP64
@@ -1350,6 +1407,23 @@ int autotune(libpt_plan *p) {
     for (int64_t x = 0; x < n; ++x) e[(size_t)x] = c.first + x;
     return e;
   };
+  {
+    // a small solve keeps the defaults: its probes (two timed runs per
+    // candidate) would cost more than a better tile could save
+    double probe = 0.0;
+    for (const SpinCase &c : p->cases)
+      probe = emu ? std::max(probe, 2.0 * ntiles *
+                                        (double)std::min<int64_t>(c.count, 4) *
+                                        c.flops_per_triple)
+                  : probe + 4.0 * (double)std::min<int64_t>(c.count, 4) *
+                                c.flops_per_triple;
+    if (probe > 0.05 * plan_flops(p, 0, (int64_t)p->queue.size())) {
+      if (tune_verbose())
+        std::fprintf(stderr, "libpt autotune %s: skipped (probes %.3g flops "
+                             "> 5%% of the solve)\n", key.c_str(), probe);
+      return LIBPT_OK;
+    }
+  }
   int r = LIBPT_OK;
   if (emu) {
     size_t big = 0;
@@ -1464,6 +1538,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       set_error("libpt_plan_create: NULL tensor argument");
       return LIBPT_ERR_ARG;
     }
+  const double t_start = wall_seconds();
   libpt_plan *p = new libpt_plan();
   p->kind = kind;
   p->unrestricted = unr;
@@ -1542,6 +1617,7 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       r = LIBPT_ERR_CUDA;
       break;
     }
+    p->prof_upload = wall_seconds() - t_start;
     if (!g_dry) {   // an all-zero f_ov (the usual case) skips its terms
       std::vector<double> f((size_t)nov);
       if (cudaMemcpy(f.data(), p->ov2, (size_t)nov * 8,
@@ -1643,8 +1719,14 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     p->ws_budget = std::min<size_t>(std::max<size_t>(fr / 2, (size_t)64 << 20),
                                     (size_t)16 << 30);
   } while (0);
+  if (!r && !g_dry && profile_enabled()) {
+    cudaStreamSynchronize(st);
+    p->prof_prepare = wall_seconds() - t_start - p->prof_upload;
+  }
+  const double t_tune = wall_seconds();
   if (!r && !g_dry && p->slices_auto) r = choose_slices(p);
   if (!r && !g_dry) r = autotune(p);
+  p->prof_tune = wall_seconds() - t_tune;
   if (r) {
     plan_destroy(p);
     return r;
@@ -1755,6 +1837,20 @@ int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e,
   if (int r = sum_slots(slots, total, idx, n, &s)) return r;
   *e = p->factor * s;
   return LIBPT_OK;
+}
+
+double wall_seconds() {
+  timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+bool profile_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("LIBPT_PROFILE");
+    return e && e[0] == '1';
+  }();
+  return on;
 }
 
 int sum_slots(const double *slots, size_t total, const int64_t *idx, size_t n,

@@ -124,6 +124,8 @@ struct libpt_plan {
   std::vector<ptb::SpinCase> cases;
   std::vector<int4> queue;              // (case, i, j, k)
   double *e_slot = nullptr;
+  // phase times of creation (s), recorded for LIBPT_PROFILE=1
+  double prof_upload = 0, prof_prepare = 0, prof_tune = 0;
   // round resources: contraction outputs (packed by each triple's own
   // size), partial energies and descriptors of one round of triples
   double *ws = nullptr;
@@ -218,6 +220,9 @@ int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e,
 // without the restricted factor; the sum libpt_plan_energy applies.
 int sum_slots(const double *slots, size_t total, const int64_t *idx, size_t n,
               double *out);
+// Monotonic wall clock (s); LIBPT_PROFILE=1 in the environment.
+double wall_seconds();
+bool profile_enabled();
 // Entries of queue length `total` that rank `rank` of `size` owns (q % size
 // == rank); writes them to idx when non-NULL; -1 for invalid arguments.
 int64_t shard_entries(int64_t total, int rank, int size, int64_t *idx);
