@@ -71,8 +71,11 @@ def parse():
     ap.add_argument("--precision", default="fp64,emu64",
                     help="comma list of fp64, emu64, tf32x3; the first is "
                          "the headline value")
-    ap.add_argument("--slices", type=int, default=6,
-                    help="emulated FP64 digit slices (4..7)")
+    ap.add_argument("--serve-slices", type=int, default=6,
+                    help="digit slices of the served stream's emulated half")
+    ap.add_argument("--slices", type=int, default=0,
+                    help="emulated FP64 digit slices (4..7; 0: chosen by the "
+                         "plan for LIBPT_EMU_TOL, default 1e-6 Eh)")
     ap.add_argument("--serve-requests", type=int, default=40,
                     help="requests of the served stream (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0,
@@ -377,11 +380,12 @@ def run_ours(args, d):
         else:
             energy = plan.energy(sample)
         n = plan.n
+        chosen = plan.slices
         plan.close()
         torch.cuda.empty_cache()
         return dict(sample=sample, flops_step=flops_step, flops_full=flops_full,
                     secs=secs, secs_max=secs_max, stats=stats, clk=clk,
-                    energy=energy, n=n, plan_seconds=t_plan,
+                    energy=energy, n=n, plan_seconds=t_plan, slices=chosen,
                     flops_all=flops_all, nsample=len(gsample),
                     nsame=int((gsample < naaa).sum()),
                     value=args.steps * flops_all / secs_max / 1e12,
@@ -498,7 +502,12 @@ def run_ours(args, d):
                 if name == "emu64" else None,
                 energy_sample=Rr["energy"],
                 energy_sample_delta=Rr["energy"] - energy_sample,
-                slices=args.slices if name == "emu64" else None,
+                slices=Rr["slices"] if name == "emu64" else None,
+                slice_choice=("chosen by the plan for |dE| <= "
+                              f"{os.environ.get('LIBPT_EMU_TOL', '1e-6')} Eh "
+                              "(sampled error estimate)")
+                if name == "emu64" and args.slices == 0 else
+                (f"fixed at {args.slices}" if name == "emu64" else None),
                 epilogue_ms_share=Rr["stats"]["epi_ms"] / max(Rr["secs"] * 1e3, 1e-9),
                 plan_seconds=Rr["plan_seconds"], clocks=Rr["clk"])
         print(json.dumps(line))
@@ -533,7 +542,7 @@ def run_serving(args, torch, gpu_id):
     service times)."""
     from libpt_b200 import ffi, synth
     reqs = serve_stream(args.serve_requests, args.serve_rate, seed=4)
-    emu = ffi.PREC_EMU64 | (args.slices << 8)
+    emu = ffi.PREC_EMU64 | (args.serve_slices << 8)
     budget = int(args.serve_budget_gb * (1 << 30))
     free = torch.cuda.mem_get_info()[0]
     # room beside the pool for arriving requests' inputs until admission
@@ -584,7 +593,7 @@ def run_serving(args, torch, gpu_id):
     return dict(
         workload=f"{len(reqs)} restricted (T) requests, o~U{{4..24}}, "
                  f"v=round(o*U[6,12]), Poisson {args.serve_rate:g} req/s, "
-                 f"half FP64 / half emulated FP64 ({args.slices} slices), "
+                 f"half FP64 / half emulated FP64 ({args.serve_slices} slices), "
                  "inputs generated on the device at arrival",
         solves_per_s=len(reqs) / wall, p50_s=percentile(lat, 50),
         p99_s=percentile(lat, 99), tflops=flops / wall / 1e12,

@@ -1311,19 +1311,29 @@ int set_bm(SpinCase &c, int bm) {
 // Emulated FP64 with the slice count left to the library: the digit planes
 // are built with the most slices (7), whose first S planes are exactly the
 // S-slice decomposition (digits come from the running remainder), so any
-// S <= 7 runs on them.  A sample of up to 16 triples spread over the queue
-// is evaluated with 7 slices and with 4, 5, 6; the error of the whole solve
-// with S slices is bounded by (queue / sample) * sum over the sample of
-// |e_S - e_7| (no cancellation assumed), and the smallest S whose bound is
-// under half the tolerance (LIBPT_EMU_TOL, default 1e-6 Eh) is kept.
+// S <= 7 runs on them.
+//
+// Error model.  Digits are rounded to nearest, so the dropped digit products
+// of a contraction element are zero-mean and their signs vary from element
+// to element; the first-order energy error of a triple, sum (2W - V) dW / D,
+// is then zero-mean, and triples (different amplitude rows) err
+// independently.  The solve's error with S slices is therefore a sum of N
+// independent per-triple errors: about sqrt(N) * rms(e_S - e_7) (the second-
+// order term sum dW^2 / D is of relative size (dW/W)^2, below 1e-18 for
+// S >= 4).  A sample of n = min(N, 16) triples spread over the queue is
+// evaluated with 7 slices and with S; the smallest S with
+//     3 sqrt(N) rms_sample(e_S - e_7) * factor <= LIBPT_EMU_TOL / 2
+// (default tolerance 1e-6 Eh) is kept.  LIBPT_EMU_BOUND=worst replaces the
+// estimate by the cancellation-free bound (N / n) sum_sample |e_S - e_7|.
+// Sampling costs about 3n triples; a solve with fewer than 40n triples
+// (where that would exceed ~8 % of the solve) keeps 7 slices unsampled.
 int choose_slices(libpt_plan *p) {
   const size_t N = p->queue.size();
   if (!N) return LIBPT_OK;
   const size_t n = std::min<size_t>(N, 16);
-  std::vector<int64_t> ents(n);
-  for (size_t t = 0; t < n; ++t) ents[t] = (int64_t)(t * N / n);
-  std::vector<double> slots(N + 1), ref(n);
-  auto run_with = [&](int S, std::vector<double> &out) -> int {
+  const char *bound_env = std::getenv("LIBPT_EMU_BOUND");
+  const bool worst = bound_env && std::strcmp(bound_env, "worst") == 0;
+  auto apply = [&](int S) -> int {
     const I8Tile *tiles = nullptr;
     if (i8_tiles(S, &tiles) <= 0) return LIBPT_ERR_ARG;
     p->slices = S;
@@ -1331,39 +1341,62 @@ int choose_slices(libpt_plan *p) {
     for (SpinCase &c : p->cases)
       if (c.count)
         if (int r = i8_encode(p, c)) return r;
-    if (int r = upload_views(p)) return r;
-    if (int r = run_entries(p, ents)) return r;
-    CK(cudaMemcpyAsync(slots.data(), p->e_slot, (N + 1) * 8,
-                       cudaMemcpyDeviceToHost, p->st));
-    CK(cudaStreamSynchronize(p->st));
-    out.resize(n);
-    for (size_t t = 0; t < n; ++t) out[t] = slots[(size_t)ents[t]];
-    return LIBPT_OK;
+    return upload_views(p);
   };
-  if (int r = run_with(TC_S_MAX, ref)) return r;
   int chosen = TC_S_MAX;
-  std::vector<double> e;
-  for (int S = TC_S_MIN; S < TC_S_MAX; ++S) {
-    if (int r = run_with(S, e)) return r;
-    double bound = 0.0;
-    for (size_t t = 0; t < n; ++t) bound += std::fabs(e[t] - ref[t]);
-    bound *= p->factor * (double)N / (double)n;
-    if (tune_verbose())
-      std::fprintf(stderr, "libpt slices: S=%d error bound %.3e Eh (target %.1e)\n",
-                   S, bound, p->emu_tol);
-    if (bound <= 0.5 * p->emu_tol) {
-      chosen = S;
-      break;
+  if (N >= 40 * n) {
+    std::vector<int64_t> ents(n);
+    for (size_t t = 0; t < n; ++t) ents[t] = (int64_t)(t * N / n);
+    std::vector<double> slots(N + 1), ref(n);
+    auto run_with = [&](int S, std::vector<double> &out) -> int {
+      if (int r = apply(S)) return r;
+      if (int r = run_entries(p, ents)) return r;
+      CK(cudaMemcpyAsync(slots.data(), p->e_slot, (N + 1) * 8,
+                         cudaMemcpyDeviceToHost, p->st));
+      CK(cudaStreamSynchronize(p->st));
+      out.resize(n);
+      for (size_t t = 0; t < n; ++t) out[t] = slots[(size_t)ents[t]];
+      return LIBPT_OK;
+    };
+    auto estimate = [&](const std::vector<double> &e) {
+      double sum_abs = 0.0, sum_sq = 0.0;
+      for (size_t t = 0; t < n; ++t) {
+        const double d = e[t] - ref[t];
+        sum_abs += std::fabs(d);
+        sum_sq += d * d;
+      }
+      return p->factor * (worst ? sum_abs * (double)N / (double)n
+                                : 3.0 * std::sqrt((double)N * sum_sq / (double)n));
+    };
+    if (int r = run_with(TC_S_MAX, ref)) return r;
+    // try 5 first, then 4 (if 5 passed) or 6 (if not)
+    std::vector<double> e;
+    auto passes = [&](int S, bool *ok) -> int {
+      if (int r = run_with(S, e)) return r;
+      const double est = estimate(e);
+      if (tune_verbose())
+        std::fprintf(stderr, "libpt slices: S=%d error estimate %.3e Eh "
+                             "(%s; target %.1e)\n", S, est,
+                     worst ? "cancellation-free bound" : "3 sqrt(N) rms",
+                     p->emu_tol);
+      *ok = est <= 0.5 * p->emu_tol;
+      return LIBPT_OK;
+    };
+    bool ok = false;
+    if (int r = passes(5, &ok)) return r;
+    if (ok) {
+      chosen = 5;
+      if (int r = passes(4, &ok)) return r;
+      if (ok) chosen = 4;
+    } else {
+      if (int r = passes(6, &ok)) return r;
+      if (ok) chosen = 6;
     }
+  } else if (tune_verbose()) {
+    std::fprintf(stderr, "libpt slices: %zu triples, too few to sample: 7\n",
+                 N);
   }
-  const I8Tile *tiles = nullptr;
-  i8_tiles(chosen, &tiles);
-  p->slices = chosen;
-  p->i8tile = tiles[0];
-  for (SpinCase &c : p->cases)
-    if (c.count)
-      if (int r = i8_encode(p, c)) return r;
-  if (int r = upload_views(p)) return r;
+  if (int r = apply(chosen)) return r;
   CK(cudaMemsetAsync(p->e_slot, 0, (N + 1) * 8, p->st));
   CK(cudaStreamSynchronize(p->st));
   p->launches = 0;

@@ -212,15 +212,53 @@ def test_emulated_fp64_chosen_slices_meet_1_uEh(kind, sz):
     assert abs(e - ref) <= 1e-6, (e, ref)
 
 
+@pytest.mark.parametrize("kind,sz", [("rpt", (20, 60)), ("upt", (14, 50, 12, 52)),
+                                     ("rft", (16, 40)), ("uft", (12, 30, 11, 33))])
+def test_emulated_fp64_sampled_slice_choice_meets_1_uEh(kind, sz):
+    """Queues long enough for the sampled choice (N >= 640 triples): the S
+    the error estimate picks keeps |dE| <= 1 uEh against the FP64 path
+    (which matches the reference to 1e-12 |E|), and the worst-case bound
+    never picks fewer slices than the estimate."""
+    import os
+    import subprocess
+    import sys
+    case = synth.make(kind, *sz, seed=8, fock=1e-3)
+    dev = to_dev(case)
+    p64 = ffi.Plan(case, dev)
+    p64.run()
+    e64 = p64.energy()
+    p64.close()
+    p = ffi.Plan(case, dev, precision=ffi.PREC_EMU64)
+    assert p.n >= 640
+    p.run()
+    e, s_est = p.energy(), p.slices
+    p.close()
+    assert 4 <= s_est <= 7
+    assert abs(e - e64) <= 1e-6, (s_est, e, e64)
+    code = (f"import sys; sys.path.insert(0, {os.getcwd()!r})\n"
+            "from libpt_b200 import ffi, synth\n"
+            "from tests.test_gpu_parity import to_dev\n"
+            f"case = synth.make({kind!r}, *{sz!r}, seed=8, fock=1e-3)\n"
+            "p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64)\n"
+            "print(p.slices)\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True,
+                       text=True, timeout=600,
+                       env=dict(os.environ, LIBPT_EMU_BOUND="worst"))
+    assert r.returncode == 0, r.stderr
+    assert int(r.stdout.strip().splitlines()[-1]) >= s_est
+
+
 def test_emulated_fp64_digit_prefix_equals_fixed_slices():
     """The first S of 7 stored digit planes are the S-slice decomposition:
     a plan that chose S from 7-slice planes gives the same energy as a plan
     built with S slices."""
     import os
-    case = synth.make("rpt", 6, 40, seed=8, fock=1e-3)
+    # 1012 triples: long enough for the sampled choice
+    case = synth.make("rpt", 12, 30, seed=8, fock=1e-3)
     os.environ["LIBPT_EMU_TOL"] = "1e3"          # loose: the choice is S = 4
     try:
         p = ffi.Plan(case, to_dev(case), precision=ffi.PREC_EMU64)
+        assert p.slices == 4
         p.run()
         e_auto = p.energy()
         p.close()
