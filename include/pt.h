@@ -125,8 +125,10 @@ const char *libpt_last_error(void);
  * m x k and k x n operands, against an FP64 reference computed on the device;
  * writes max|C - C_ref| / max(|A| (|B1| + |B2|)) to *rel_err (the error over
  * the scale that bounds a dot product's rounding).  precision selects the
- * kernel (LIBPT_PREC_*, with the slice count in bits 8-15 for
- * LIBPT_PREC_EMU64) and bits 16-23 a tile variant: FP64 0 = 128-row,
+ * kernel (LIBPT_PREC_*, with the slice count in bits 8-14 for
+ * LIBPT_PREC_EMU64, and bit 15 set for 8-bit digit planes -- a signed top
+ * digit, unsigned lower digits; S <= 6 -- instead of 7-bit signed digits)
+ * and bits 16-23 a tile variant: FP64 0 = 128-row,
  * 1 = 96-row tiles; emulated FP64 the index of one of the slice count's
  * INT8 tile shapes (0 = widest); libpt_selftest_variants() counts them.
  * Bits 24-31 nonzero: the kernel reads its tensor maps from device memory

@@ -51,7 +51,9 @@ struct GemmJob {
   // plans per launch, fixed kernel parameters for graph replay; kernels
   // fence each such map before first use).
   const CUtensorMap *maps;
-  int32_t map0, pad_;
+  int32_t map0;
+  // emulated FP64: digit base bits of the planes (7 or 8; 0 reads as 7)
+  int32_t dbits;
 };
 
 // Kernel-parameter table of the tensor maps of one launch (12 KiB of
@@ -242,13 +244,15 @@ cudaError_t colmax_launch(const double *src, int64_t P, int64_t K, int64_t N,
 cudaError_t exps_launch(const unsigned long long *m1,
                         const unsigned long long *m2, double s2, int64_t n,
                         signed char *e, cudaStream_t st);
+// Digit planes of base 2^bits (7: balanced digits; 8: signed top digit,
+// unsigned lower digits, the last rounded); see prep.cu.
 cudaError_t slice_a_launch(const double *src, int64_t npq, int64_t R,
                            int64_t K, int64_t kp, int64_t kpi, double scale,
-                           const signed char *ea, int S, signed char *out,
-                           cudaStream_t st);
+                           const signed char *ea, int S, int bits,
+                           signed char *out, cudaStream_t st);
 cudaError_t slice_b_launch(const double *src, int64_t P, int K, int64_t N,
                            int64_t w, int64_t wsrc, int64_t ldsrc, int64_t kpi,
-                           double scale, const signed char *eb, int S,
+                           double scale, const signed char *eb, int S, int bits,
                            signed char *out, cudaStream_t st);
 
 }  // namespace ptb

@@ -2,15 +2,17 @@
 // 5th-generation tensor cores (tcgen05.mma kind::i8), exact INT32
 // accumulation in TMEM.
 //
-// Each FP64 operand is stored as S signed 7-bit digit planes of the operand
-// scaled by a power of two per row (A) / column (B).  A tile's result is
-//     C = 2^(ea[row] + eb[col]) * sum_w acc_w 2^-7(w+2),
+// Each FP64 operand is stored as S signed INT8 digit planes of base 2^b
+// (b = 7 or 8, GemmJob::dbits) of the operand scaled by a power of two per
+// row (A) / column (B).  A tile's result is
+//     C = 2^(ea[row] + eb[col]) * g * sum_w acc_w 2^-b(w+2),
 //     acc_w = sum over digit pairs p + q = w (w <= S-1) of dA_p dB_q,
+// (g = 1 for b = 7; g = 4 for b = 8, whose digits carry a factor 2 each),
 // each acc_w an exact INT32 sum in its own TMEM accumulator (S accumulators
-// of BN columns; S * BN <= 512).  Subtracted segments read the negated
-// digit planes (stored after the digit planes; GemmSeg::neg holds their
+// of BN columns; S * BN <= 512).  Subtracted segments read the planes of the
+// negated operand (stored after the digit planes; GemmSeg::neg holds their
 // first plane), so all products accumulate with +.  The kernel may use the
-// first S of more stored planes (the digits of a shorter decomposition).
+// first S of more stored planes.
 //
 // Tile variants (BN columns, KC = 32 or 64 bytes of K per pipeline stage):
 // an M=128 INT8 MMA reads (128 + BN) * 32 bytes of shared memory per
@@ -251,7 +253,7 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
                   kmajor_desc<32>(sa + pa * C::A_TILE + kk * C::A_SUB);
 #pragma unroll
               for (int pb = 0; pb + pa < S; ++pb) {
-                const int w = pa + pb;     // digit weight 2^-7(w+2)
+                const int w = pa + pb;     // digit weight 2^-b(w+2)
                 const uint64_t db =
                     kmajor_desc<32>(sb + pb * C::B_TILE + kk * C::B_SUB);
                 mma_i8(tmem + (uint32_t)(w * BN), da, db, i8_idesc<BN>(),
@@ -275,11 +277,13 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
     const int half = (warp - 2) >> 2;  // which 16-column chunks it takes
     int it = 0;
     constexpr int H = C::H;
-    // weights of the two partial sums: hi counts units of acc_{H-1},
-    // lo units of acc_{S-1}
-    const double w_hi = pow2i(-7 * (H + 1)), w_lo = pow2i(-7 * (S + 1));
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
       const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
+      // digit base 2^b; weights of the two partial sums: hi counts units of
+      // acc_{H-1}, lo units of acc_{S-1}
+      const int b = job.dbits == 8 ? 8 : 7, g = b == 8 ? 2 : 0;
+      const long long base = 1ll << b;
+      const double w_hi = pow2i(g - b * (H + 1)), w_lo = pow2i(g - b * (S + 1));
       const int local = tile - job.tile_begin;
       const int m0 = (local % job.mtiles) * BM;
       const int n0 = (local / job.mtiles) * BN;
@@ -295,7 +299,9 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
 #pragma unroll 1
       for (int c0 = 16 * half; c0 < BN; c0 += 32) {
         // exact: acc_0..acc_{H-1} and acc_H..acc_{S-1} folded by Horner in
-        // base 2^7 into 64-bit integers (|sum| < 2^50 for |acc| < 2^28)
+        // base 2^b into 64-bit integers; |acc| < 2^31 and each sum has at
+        // most 4 terms of base 2^7 or 3 of base 2^8 (8-bit digits only for
+        // S <= 6), so |sum| < 2^53 and its conversion to double is exact
         long long hi[16], lo[16];
         {
           uint32_t r[H][16];
@@ -306,7 +312,7 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
           for (int x = 0; x < 16; ++x) {
             long long h = (int)r[0][x];
 #pragma unroll
-            for (int a = 1; a < H; ++a) h = h * 128 + (int)r[a][x];
+            for (int a = 1; a < H; ++a) h = h * base + (int)r[a][x];
             hi[x] = h;
           }
         }
@@ -319,7 +325,7 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
           for (int x = 0; x < 16; ++x) {
             long long l = (int)r[0][x];
 #pragma unroll
-            for (int a = H + 1; a < S; ++a) l = l * 128 + (int)r[a - H][x];
+            for (int a = H + 1; a < S; ++a) l = l * base + (int)r[a - H][x];
             lo[x] = l;
           }
         }

@@ -975,6 +975,7 @@ int i8_encode(libpt_plan *p, SpinCase &c) {
   return LIBPT_OK;
 }
 
+// Digit planes of a case's operands (shared between cases by source).
 int i8_planes(libpt_plan *p, SpinCase &c) {
   const int S = p->slices_store;
   for (int i = 0; i < MAX_MAPS; ++i) {
@@ -990,20 +991,18 @@ int i8_planes(libpt_plan *p, SpinCase &c) {
     for (auto &e : p->i8planes)
       if (e.first == key) pl = e.second;
     if (!pl) {
-      if (d.role == 0) {
-        const int64_t n = d.P * d.Q * d.R * kpi;
-        if (dalloc(p, (void **)&pl, 2 * S * n)) return LIBPT_ERR_NOMEM;
-        DEV(slice_a_launch(d.src, d.P * d.Q, d.R, d.K, pad4(d.K), kpi,
-                          std::ldexp(1.0, d.part ? -k : 0), f->e, S, pl,
-                          p->st));
-      } else {
-        const int64_t n = d.P * d.N * kpi;
-        if (dalloc(p, (void **)&pl, S * n)) return LIBPT_ERR_NOMEM;
-        DEV(slice_b_launch(d.src, d.P, (int)d.K, d.N, d.w, d.wsrc, d.ldsrc, kpi,
-                          std::ldexp(1.0, d.part ? k : 0), f->e, S, pl,
-                          p->st));
-      }
+      const int64_t n = d.role == 0 ? d.P * d.Q * d.R * kpi : d.P * d.N * kpi;
+      if (dalloc(p, (void **)&pl, (d.role == 0 ? 2 : 1) * S * n))
+        return LIBPT_ERR_NOMEM;
       p->i8planes.push_back({key, pl});
+      if (d.role == 0)
+        DEV(slice_a_launch(d.src, d.P * d.Q, d.R, d.K, pad4(d.K), kpi,
+                          std::ldexp(1.0, d.part ? -k : 0), f->e, S, p->dbits,
+                          pl, p->st));
+      else
+        DEV(slice_b_launch(d.src, d.P, (int)d.K, d.N, d.w, d.wsrc, d.ldsrc, kpi,
+                          std::ldexp(1.0, d.part ? k : 0), f->e, S, p->dbits,
+                          pl, p->st));
     }
     c.i8pl[i] = pl;
   }
@@ -1014,6 +1013,44 @@ int i8_planes(libpt_plan *p, SpinCase &c) {
       if (f.id == c.opd[j.seg[0].amap].fam) j.ea = f.e;
       if (f.id == c.opd[j.seg[0].bmap].fam) j.eb = f.e;
     }
+  }
+  return LIBPT_OK;
+}
+
+// Digit width of the INT8 planes.  Every accumulator (one digit-weight
+// diagonal: at most S digit products per unit of K, summed over a job's
+// segments) must stay below 2^31: S * 64^2 per unit of K for 7-bit digits,
+// S * 128^2 for 8-bit ones.  8-bit digits (8 bits of the operand per lower
+// plane instead of 7) are used for S <= 6 whenever they fit, unless
+// LIBPT_EMU_DIGITS=7; a plan that chooses S itself then stores 6 planes
+// (47 bits, about as accurate as 7 planes of 7 bits).
+int choose_digits(libpt_plan *p) {
+  int64_t kmax = 0;
+  for (const SpinCase &c : p->cases)
+    for (const JobT &j : c.jobs) {
+      int64_t k = 0;
+      for (int s = 0; s < j.nseg; ++s) k += j.seg[s].k;
+      kmax = std::max(kmax, k);
+    }
+  const char *env = std::getenv("LIBPT_EMU_DIGITS");
+  const bool allow8 = !(env && std::atoi(env) == 7);
+  auto fits8 = [&](int S) {
+    return allow8 && S <= 6 && (double)kmax * S * 16384.0 < 2147483648.0;
+  };
+  if (p->slices_auto) {
+    const int S = fits8(6) ? 6 : TC_S_MAX;
+    p->dbits = S == 6 ? 8 : 7;
+    p->slices = p->slices_store = S;
+    const I8Tile *t = nullptr;
+    if (i8_tiles(S, &t) > 0) p->i8tile = t[0];
+  } else {
+    p->dbits = fits8(p->slices_store) ? 8 : 7;
+  }
+  if (p->dbits == 7 &&
+      (double)kmax * 4096.0 * p->slices_store >= 2147483648.0) {
+    set_error("emulated FP64: contraction too long for exact INT32 "
+              "accumulation");
+    return LIBPT_ERR_UNSUPPORTED;
   }
   return LIBPT_OK;
 }
@@ -1066,6 +1103,7 @@ int add_cases(libpt_plan *p) {
     if (r) return r;
   }
   if (p->precision == LIBPT_PREC_EMU64) {
+    if (int r = choose_digits(p)) return r;
     if (int r = i8_maxima(p)) return r;
     if (int r = i8_exponents(p)) return r;
     for (SpinCase &c : p->cases)
@@ -1205,6 +1243,7 @@ int plan_append(libpt_plan *p, const int64_t *ents, size_t n, PlanCursor &cur,
       g.eb = jt.eb;
       g.maps = c.d_maps;
       g.map0 = map0;
+      g.dbits = i8 ? p->dbits : 0;
       g.ntiles_n = (jt.N + bn - 1) / bn;
       g.mtiles = (jt.M + bmr - 1) / bmr;
       g.nseg = jt.nseg;
@@ -1309,9 +1348,10 @@ int set_bm(SpinCase &c, int bm) {
 }
 
 // Emulated FP64 with the slice count left to the library: the digit planes
-// are built with the most slices (7), whose first S planes are exactly the
-// S-slice decomposition (digits come from the running remainder), so any
-// S <= 7 runs on them.
+// are built with the most slices (6 of 8 bits, or 7 of 7 bits; see
+// choose_digits) and any S below runs on their first S planes, which are
+// the S-digit decomposition (with 8-bit digits, but for rare carries into
+// the last kept digit, which stay within the same error bound).
 //
 // Error model.  Digits are rounded to nearest, so the dropped digit products
 // of a contraction element are zero-mean and their signs vary from element
@@ -1321,12 +1361,12 @@ int set_bm(SpinCase &c, int bm) {
 // independent per-triple errors: about sqrt(N) * rms(e_S - e_7) (the second-
 // order term sum dW^2 / D is of relative size (dW/W)^2, below 1e-18 for
 // S >= 4).  A sample of n = min(N, 16) triples spread over the queue is
-// evaluated with 7 slices and with S; the smallest S with
-//     3 sqrt(N) rms_sample(e_S - e_7) * factor <= LIBPT_EMU_TOL / 2
+// evaluated with all stored planes (e_max) and with S; the smallest S with
+//     3 sqrt(N) rms_sample(e_S - e_max) * factor <= LIBPT_EMU_TOL / 2
 // (default tolerance 1e-6 Eh) is kept.  LIBPT_EMU_BOUND=worst replaces the
-// estimate by the cancellation-free bound (N / n) sum_sample |e_S - e_7|.
+// estimate by the cancellation-free bound (N / n) sum_sample |e_S - e_max|.
 // Sampling costs about 3n triples; a solve with fewer than 40n triples
-// (where that would exceed ~8 % of the solve) keeps 7 slices unsampled.
+// (where that would exceed ~8 % of the solve) keeps all stored planes.
 int choose_slices(libpt_plan *p) {
   const size_t N = p->queue.size();
   if (!N) return LIBPT_OK;
@@ -1343,7 +1383,8 @@ int choose_slices(libpt_plan *p) {
         if (int r = i8_encode(p, c)) return r;
     return upload_views(p);
   };
-  int chosen = TC_S_MAX;
+  const int smax = p->slices_store;   // 6 (8-bit digits) or 7 (7-bit)
+  int chosen = smax;
   if (N >= 40 * n) {
     std::vector<int64_t> ents(n);
     for (size_t t = 0; t < n; ++t) ents[t] = (int64_t)(t * N / n);
@@ -1368,8 +1409,8 @@ int choose_slices(libpt_plan *p) {
       return p->factor * (worst ? sum_abs * (double)N / (double)n
                                 : 3.0 * std::sqrt((double)N * sum_sq / (double)n));
     };
-    if (int r = run_with(TC_S_MAX, ref)) return r;
-    // try 5 first, then 4 (if 5 passed) or 6 (if not)
+    if (int r = run_with(smax, ref)) return r;
+    // try 5 first, then 4 (if 5 passed) or 6 (if not, and 6 < smax)
     std::vector<double> e;
     auto passes = [&](int S, bool *ok) -> int {
       if (int r = run_with(S, e)) return r;
@@ -1388,13 +1429,13 @@ int choose_slices(libpt_plan *p) {
       chosen = 5;
       if (int r = passes(4, &ok)) return r;
       if (ok) chosen = 4;
-    } else {
+    } else if (smax > 6) {
       if (int r = passes(6, &ok)) return r;
       if (ok) chosen = 6;
     }
   } else if (tune_verbose()) {
-    std::fprintf(stderr, "libpt slices: %zu triples, too few to sample: 7\n",
-                 N);
+    std::fprintf(stderr, "libpt slices: %zu triples, too few to sample: %d\n",
+                 N, smax);
   }
   if (int r = apply(chosen)) return r;
   CK(cudaMemsetAsync(p->e_slot, 0, (N + 1) * 8, p->st));

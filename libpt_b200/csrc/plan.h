@@ -151,6 +151,7 @@ struct libpt_plan {
   // emulated FP64: digit planes per (source block, role), scale families
   int slices = 6;                       // digit planes the kernels use
   int slices_store = 6;                 // digit planes stored (>= slices)
+  int dbits = 7;                        // digit base bits of the planes (7, 8)
   bool slices_auto = false;             // choose slices for emu_tol
   double emu_tol = 1e-6;                // |dE| target of the choice (Eh)
   ptb::I8Tile i8tile{64, 32};           // emulated FP64 tile variant

@@ -158,13 +158,24 @@ cudaError_t transpose_split_tf32_launch(const double *src, float *hi,
 
 }  // namespace ptb
 
-// ---- emulated FP64: power-of-two scales and signed 7-bit digit planes ----
+// ---- emulated FP64: power-of-two scales and digit planes ----------------
 //
-// An operand value a with scale exponent e is written as
-//   a * 2^-e = sum_{p=1..S} d_p 2^-7p (+ remainder < 2^-7S / 2),  |d_p| <= 64,
-// digits by round-to-nearest of the running remainder (Ozaki-style slicing;
-// all steps exact in FP64).  e is chosen per A row / B column as
-// ceil-log2(max |a|) + 1, so |a 2^-e| <= 1/2.
+// An operand value a with scale exponent e (chosen per A row / B column as
+// ceil-log2(max |a|) + 1, so |a 2^-e| < 1/2) is written in S base-2^b digits
+//   a * 2^-e = sum_{p=1..S} d_p 2^-bp + remainder,
+// every step exact in FP64 (Ozaki-style slicing).  Two digit forms:
+//   b = 7: balanced digits |d_p| <= 64, each rounded to nearest from the
+//          running remainder (|remainder| <= 2^-7S / 2); any first S' of the
+//          S digits are the S'-digit decomposition.
+//   b = 8: balanced digits of base 2^8, value 2 sum_p d_p 2^-8p: the top
+//          digit rint(128 s) in [-64, 64], each lower digit rint(256 r) of
+//          the running remainder, a digit 128 replaced by -128 with a carry
+//          of 1 into the digit above (the top digit then stays <= 65), so
+//          every digit fits a signed byte, |remainder| <= 2^-8S (in units
+//          of s) and the truncation is unbiased; 8 bits of the operand per
+//          lower plane instead of 7.  A prefix of S' digits is the S'-digit
+//          decomposition but where a carry from below changed its last
+//          digit (its error then stays within 2^-8S' (1 + 2^-7)).
 
 namespace ptb {
 
@@ -231,13 +242,34 @@ __global__ void exps_kernel(const unsigned long long *m1,
   }
 }
 
-__device__ __forceinline__ void digits(double s, int S, signed char *d) {
+__device__ __forceinline__ void digits7(double s, int S, signed char *d) {
   for (int q = 0; q < S; ++q) {
     const double t = s * 128.0;
     const double r = rint(t);
     d[q] = (signed char)r;
     s = t - r;
   }
+}
+
+// s in (-1/2, 1/2): s = 2 sum_{q<S} d[q] 2^-8(q+1) + remainder.
+__device__ __forceinline__ void digits8(double s, int S, signed char *d) {
+  int v[8];
+  double t = s * 128.0;
+  double f = rint(t);
+  v[0] = (int)f;
+  s = t - f;                       // |s| <= 1/2
+  for (int q = 1; q < S; ++q) {
+    t = s * 256.0;
+    f = rint(t);
+    v[q] = (int)f;                 // in [-128, 128]
+    s = t - f;
+  }
+  for (int q = S - 1; q >= 1; --q)
+    if (v[q] == 128) {             // 128 * 2^-8q = -128 * 2^-8q + 2^-8(q-1)
+      v[q] = -128;
+      v[q - 1] += 1;
+    }
+  for (int q = 0; q < S; ++q) d[q] = (signed char)v[q];
 }
 
 // A side: src[npq][R][kp] (FP64) -> out[2S][npq][kpi/32][R][32] int8: digit
@@ -247,19 +279,26 @@ __device__ __forceinline__ void digits(double s, int S, signed char *d) {
 __global__ void slice_a_kernel(const double *__restrict__ src, int64_t npq,
                                int64_t R, int64_t K, int64_t kp, int64_t kpi,
                                double scale, const signed char *ea, int S,
-                               signed char *__restrict__ out) {
+                               int bits, signed char *__restrict__ out) {
   const int64_t n = npq * R * kpi, plane = n;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t rr = i / kpi, k = i - rr * kpi;
     const int64_t pq = rr / R, r = rr - pq * R;
     const double a = k < K ? src[rr * kp + k] : 0.0;
-    signed char d[8];
-    digits(ldexp(a * scale, -ea[r]), S, d);
+    const double x = ldexp(a * scale, -ea[r]);
+    signed char d[8], nd[8];
+    if (bits == 8) {
+      digits8(x, S, d);
+      digits8(-x, S, nd);   // -(-128) does not fit a signed byte
+    } else {
+      digits7(x, S, d);
+      for (int q = 0; q < S; ++q) nd[q] = (signed char)(-d[q]);
+    }
     const int64_t o = pq * R * kpi + ((k >> 5) * R + r) * 32 + (k & 31);
     for (int q = 0; q < S; ++q) {
       out[q * plane + o] = d[q];
-      out[(S + q) * plane + o] = (signed char)(-d[q]);
+      out[(S + q) * plane + o] = nd[q];
     }
   }
 }
@@ -270,8 +309,8 @@ __global__ void slice_a_kernel(const double *__restrict__ src, int64_t npq,
 __global__ void slice_b_kernel(const double *__restrict__ src, int K,
                                int64_t N, int64_t w, int64_t wsrc,
                                int64_t ldsrc, int64_t kpi, double scale,
-                               const signed char *eb, int S, int64_t P,
-                               signed char *__restrict__ out) {
+                               const signed char *eb, int S, int bits,
+                               int64_t P, signed char *__restrict__ out) {
   __shared__ double t[32][33];
   const int64_t p = blockIdx.z;
   const int64_t n0 = (int64_t)blockIdx.x * 32;
@@ -290,7 +329,11 @@ __global__ void slice_b_kernel(const double *__restrict__ src, int K,
     const int k = k0 + threadIdx.x;
     if (n < N && k < kpi) {
       signed char d[8];
-      digits(ldexp(t[threadIdx.x][rr] * scale, -eb[n]), S, d);
+      const double x = ldexp(t[threadIdx.x][rr] * scale, -eb[n]);
+      if (bits == 8)
+        digits8(x, S, d);
+      else
+        digits7(x, S, d);
       const int64_t o = p * N * kpi + ((int64_t)(k >> 5) * N + n) * 32 + (k & 31);
       for (int q = 0; q < S; ++q) out[q * plane + o] = d[q];
     }
@@ -337,27 +380,29 @@ cudaError_t exps_launch(const unsigned long long *m1,
 
 cudaError_t slice_a_launch(const double *src, int64_t npq, int64_t R,
                            int64_t K, int64_t kp, int64_t kpi, double scale,
-                           const signed char *ea, int S, signed char *out,
-                           cudaStream_t st) {
+                           const signed char *ea, int S, int bits,
+                           signed char *out, cudaStream_t st) {
   if (npq * R <= 0) return cudaSuccess;
+  if (bits != 7 && bits != 8) return cudaErrorInvalidValue;
   slice_a_kernel<<<grid2(npq * R * kpi), 256, 0, st>>>(src, npq, R, K, kp, kpi,
-                                                       scale, ea, S, out);
+                                                       scale, ea, S, bits, out);
   return cudaGetLastError();
 }
 
 cudaError_t slice_b_launch(const double *src, int64_t P, int K, int64_t N,
                            int64_t w, int64_t wsrc, int64_t ldsrc, int64_t kpi,
                            double scale, const signed char *eb, int S,
-                           signed char *out, cudaStream_t st) {
+                           int bits, signed char *out, cudaStream_t st) {
   if (P <= 0 || N <= 0 || kpi <= 0) return cudaSuccess;
+  if (bits != 7 && bits != 8) return cudaErrorInvalidValue;
   for (int64_t p0 = 0; p0 < P; p0 += 65535) {
     const int64_t np_ = P - p0 < 65535 ? P - p0 : 65535;
     dim3 grid((unsigned)((N + 31) / 32), (unsigned)((kpi + 31) / 32),
               (unsigned)np_);
     // planes keep their full [P] extent: offset the output by p0 rows
     slice_b_kernel<<<grid, dim3(32, 8), 0, st>>>(
-        src + p0 * K * ldsrc, K, N, w, wsrc, ldsrc, kpi, scale, eb, S, P,
-        out + p0 * N * kpi);
+        src + p0 * K * ldsrc, K, N, w, wsrc, ldsrc, kpi, scale, eb, S, bits,
+        P, out + p0 * N * kpi);
   }
   return cudaGetLastError();
 }

@@ -73,7 +73,8 @@ namespace {
 int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
                 double *ms) {
   using namespace ptb;
-  int slices = (precision >> 8) & 0xFF;
+  int slices = (precision >> 8) & 0x7F;
+  const int dbits = (precision >> 15) & 1 ? 8 : 7;   // digit width
   const int variant = (precision >> 16) & 0xFF;
   const bool dev_maps = ((precision >> 24) & 0xFF) != 0;
   precision &= 0xFF;
@@ -86,7 +87,10 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
   if (!rel_err || m < 1 || n < 1 || k < 1 || m > 4096 || n > (1 << 20) ||
       k > 4096 || (int64_t)n * k > ((int64_t)1 << 27) ||
       (int64_t)m * n > ((int64_t)1 << 25) || reps < 0 ||
-      slices < TC_S_MIN || slices > TC_S_MAX ||
+      slices < TC_S_MIN || slices > TC_S_MAX || (dbits == 8 && slices > 6) ||
+      // 8-bit digits: the two segments' 2k products per diagonal stay
+      // below 2^31 (see choose_digits in plan.cu)
+      (dbits == 8 && 2.0 * k * slices * 16384.0 >= 2147483648.0) ||
       (precision != LIBPT_PREC_FP64 && precision != LIBPT_PREC_TF32X3 &&
        precision != LIBPT_PREC_EMU64) || variant >= nvar) {
     set_error("libpt_selftest: bad arguments");
@@ -199,10 +203,13 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
         (ce = colmax_launch(B2, 1, k, np, np, np, np, mb1, nullptr)) ||
         (ce = exps_launch(ma, nullptr, 1.0, m, ea, nullptr)) ||
         (ce = exps_launch(mb0, mb1, 1.0, np, eb, nullptr)) ||
-        (ce = slice_a_launch(A, 1, m, k, kp, kpi, 1.0, ea, S, pa, nullptr)) ||
-        (ce = slice_b_launch(B1, 1, k, np, np, np, np, kpi, 1.0, eb, S, pb1,
+        (ce = slice_a_launch(A, 1, m, k, kp, kpi, 1.0, ea, S, dbits, pa,
                              nullptr)) ||
-        (ce = slice_b_launch(B2, 1, k, np, np, np, np, kpi, 1.0, eb, S, pb2,
+        (ce = slice_b_launch(B1, 1, k, np, np, np, np, kpi, 1.0, eb, S, dbits,
+                             pb1,
+                             nullptr)) ||
+        (ce = slice_b_launch(B2, 1, k, np, np, np, np, kpi, 1.0, eb, S, dbits,
+                             pb2,
                              nullptr))) {
       set_error(cudaGetErrorString(ce));
       return done(LIBPT_ERR_CUDA);
@@ -216,6 +223,7 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
     job.ntiles_n = (int)((np + tl.bn - 1) / tl.bn);
     job.ea = ea;
     job.eb = eb;
+    job.dbits = dbits;
     const int kc = tl.kc;
     for (int s2 = 0; s2 < 2; ++s2) {
       job.seg[s2].amap = 0;
@@ -346,7 +354,7 @@ LIBPT_API int libpt_kernel_bench(int precision, int m, int n, int k, int reps,
 }
 
 LIBPT_API int libpt_selftest_variants(int precision) {
-  int slices = (precision >> 8) & 0xFF;
+  int slices = (precision >> 8) & 0x7F;
   if (slices == 0) slices = 6;
   switch (precision & 0xFF) {
     case LIBPT_PREC_FP64: return 2;

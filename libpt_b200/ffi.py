@@ -165,12 +165,15 @@ def solve_device(case, tensors, mp=False, stream=None):
     return e.value
 
 
-def selftest(precision, m, n, k, variant=0, device_maps=False):
+def selftest(precision, m, n, k, variant=0, device_maps=False, dbits=7):
     """Error of one contraction kernel (tile variant `variant`; tensor maps
-    from device memory when device_maps) against an FP64 product, over the
-    dot products' magnitude scale (libpt_selftest)."""
+    from device memory when device_maps; emulated FP64 digit width dbits)
+    against an FP64 product, over the dot products' magnitude scale
+    (libpt_selftest)."""
     e = ctypes.c_double(-1.0)
     word = precision | (variant << 16) | ((1 << 24) if device_maps else 0)
+    if dbits == 8:
+        word |= 1 << 15
     check(lib().libpt_selftest(word, m, n, k, ctypes.byref(e)))
     return e.value
 

@@ -29,6 +29,9 @@ def test_tcgen05_tf32x3(m, n, k):
 # operand's truncation 2^(-7S-1); with row / column scales up to 4x the
 # values, the error over sum |a||b| stays below 2^(-7S+6)
 EMU_BOUND = {s: 2.0 ** (-7 * s + 6) for s in (4, 5, 6, 7)}
+# 8-bit balanced digits (a 7-bit top digit, 8 bits per lower digit): each
+# operand's truncation 2^(-8S) instead of 2^(-7S-1), the same terms besides
+EMU8_BOUND = {s: 2.0 ** (-8 * s + 8) for s in (4, 5, 6)}
 
 
 # every compiled INT8 tile variant (tile width x K chunk) of each slice count
@@ -45,6 +48,19 @@ def test_tcgen05_int8_emulated_fp64(slices, variant, m, n, k):
     assert ffi.selftest(prec, m, n, k, variant) < EMU_BOUND[slices]
 
 
+@pytest.mark.parametrize("slices,variant",
+                         [(s, t) for s, n in I8_VARIANTS.items() if s <= 6
+                          for t in range(n)])
+@pytest.mark.parametrize("m,n,k", SHAPES[1:])
+def test_tcgen05_int8_emulated_fp64_8bit_digits(slices, variant, m, n, k):
+    """8-bit balanced digit planes (carries into the digit above)."""
+    prec = ffi.PREC_EMU64 | (slices << 8)
+    e8 = ffi.selftest(prec, m, n, k, variant, dbits=8)
+    assert e8 < EMU8_BOUND[slices]
+    if slices <= 5 and m * n >= 10000:   # the extra bit per plane shows
+        assert e8 < ffi.selftest(prec, m, n, k, variant)
+
+
 @pytest.mark.parametrize("m,n,k", [(5, 7, 3), (300, 520, 700)])
 def test_device_memory_tensor_maps(m, n, k):
     """The form batched multi-solve launches use: tensor maps read from
@@ -54,3 +70,5 @@ def test_device_memory_tensor_maps(m, n, k):
     for s in (4, 6):
         prec = ffi.PREC_EMU64 | (s << 8)
         assert ffi.selftest(prec, m, n, k, 0, device_maps=True) < EMU_BOUND[s]
+        assert ffi.selftest(prec, m, n, k, 0, device_maps=True,
+                            dbits=8) < EMU8_BOUND[s]
