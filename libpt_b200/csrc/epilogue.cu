@@ -83,7 +83,7 @@ __device__ __forceinline__ void load_args(EpiArgs &dst, const EpiArgs *src) {
 }
 
 template <bool FT, bool LOOP>
-__global__ void __launch_bounds__(EPI_THREADS, 2)
+__global__ void __launch_bounds__(EPI_THREADS, 3)
     epi_aaa_kernel(const EpiList *__restrict__ list) {
   extern __shared__ double sm[];
   __shared__ EpiArgs p;
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
 // ---------------------------------------------------------------- aab ----
 
 template <bool FT, bool LOOP>
-__global__ void __launch_bounds__(EPI_THREADS, 2)
+__global__ void __launch_bounds__(EPI_THREADS, 3)
     epi_aab_kernel(const EpiList *__restrict__ list) {
   extern __shared__ double sm[];
   __shared__ EpiArgs p;
@@ -288,6 +288,15 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
   const double f_ia = u2[i * va + ac], f_ja = u2[j * va + ac];
   const double o1k = p.ov1_b[k * vb + cc], o2k = p.ov2_b[k * vb + cc];
   const double dia = p.d_a[i * va + ac], dkc = p.d_b[k * vb + cc];
+  // U1 in both orientations, loaded before the wait for the staged
+  // operands so that the two sets of loads are in flight together (the
+  // wait is a memory barrier for the compiler)
+  double xu[EPI_B];
+#pragma unroll
+  for (int b_ = 0; b_ < EPI_B; ++b_) {
+    const int bc = b0 + b_ < va ? b0 + b_ : va - 1;
+    xu[b_] = U1[ac * ld1 + bc * r1 + cc] - U1[bc * ld1 + ac * r1 + cc];
+  }   // offsets < 2^31 (checked by the plan)
   cp_async_wait_all();
   __syncthreads();
 
@@ -298,11 +307,11 @@ __global__ void __launch_bounds__(EPI_THREADS, 2)
     const int b = b0 + b_;
     const bool ok = a < va && b < a && c < vb;
     const int bc = b < va ? b : va - 1;
-    const int u_ab = ac * ld1 + bc * r1 + cc;   // < 2^31 (checked by
-    const int u_ba = bc * ld1 + ac * r1 + cc;   // the plan)
+    const int u_ab = ac * ld1 + bc * r1 + cc;
+    const int u_ba = bc * ld1 + ac * r1 + cc;
     const int ix = (a_ * EPI_B + b_) * EPI_CS + lane;
     const int iy = (b_ * EPI_A + a_) * EPI_CS + lane;
-    const double w = U1[u_ab] + sx[ix] - U1[u_ba] - sy[iy] + sp[ix];
+    const double w = xu[b_] + sx[ix] - sy[iy] + sp[ix];
     const double rr = FT ? U1r[u_ab] + sx[3 * S + ix] - U1r[u_ba] -
                                sy[3 * S + iy] + sp[3 * S + ix]
                          : w;
