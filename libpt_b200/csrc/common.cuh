@@ -114,6 +114,53 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map,
       : "memory");
 }
 
+// ---- CTA pairs (clusters of two) -------------------------------------------
+
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// All threads of both CTAs of the cluster.
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile(
+      "barrier.cluster.arrive.release.aligned;\n\t"
+      "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Shared::cluster address of the same shared-memory location in CTA `rank`.
+__device__ __forceinline__ uint32_t cluster_addr(const void *p, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+               : "=r"(a)
+               : "r"(smem_u32(p)), "r"(rank));
+  return a;
+}
+
+// Arrive on an mbarrier of either CTA of the cluster (shared::cluster
+// address).
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar) {
+  asm volatile(
+      "mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar)
+      : "memory");
+}
+
+// 5-D tiled TMA load into this CTA's shared memory whose completion is
+// counted on an mbarrier of either CTA of the pair (no multicast).
+__device__ __forceinline__ void tma_load_5d_pair(void *dst,
+                                                 const CUtensorMap *map,
+                                                 uint32_t bar, int c0, int c1,
+                                                 int c2, int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.cta_group::2.shared::cluster.global.mbarrier::"
+      "complete_tx::bytes [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c0), "r"(c1),
+      "r"(c2), "r"(c3), "r"(c4)
+      : "memory");
+}
+
 // Makes a tensor map that generic-proxy writes (a host copy, or a previous
 // plan's maps at the same address) put in device memory visible to the TMA
 // unit's tensor-map proxy; issued once per map before this CTA's first TMA

@@ -133,11 +133,20 @@ cudaError_t gemm_tc_launch(const GemmJob *d_jobs, const GemmList *d_list,
 // and swizzled to 32 bytes.  An A segment's (Q, P) coordinates are merged
 // into a_q = a_p * Q + a_q.
 struct I8Tile {
-  int bn;   // tile columns (multiple of 16, S * bn <= 512)
-  int kc;   // K bytes per pipeline stage (32 or 64: one or two MMA K steps)
+  int bn;     // tile columns (multiple of 16, S * bn <= 512)
+  int kc;     // K bytes per pipeline stage (I8_KCHUNK: two MMA K steps)
+  int pair;   // 1: a CTA pair (two SMs) computes a 256 x bn tile, each CTA
+              // loading its 128 rows of A and half of the bn columns of B
+  int ts;     // 1: the MMAs read A from TMEM (copied there once per plane
+              // and K step) instead of re-reading it from shared memory
 };
-// K padded to whole 32-byte chunks: the row extent of the digit planes.
-inline int64_t i8_kpad(int64_t K) { return (K + 31) & ~int64_t(31); }
+// Digit planes are stored in K chunks of I8_KCHUNK bytes (64: one 64-byte
+// swizzled row per TMA box row; a box of R rows is one contiguous block).
+constexpr int I8_KCHUNK = 64;
+// K padded to whole chunks: the row extent of the digit planes.
+inline int64_t i8_kpad(int64_t K) {
+  return (K + I8_KCHUNK - 1) & ~int64_t(I8_KCHUNK - 1);
+}
 // The tile variants compiled for a slice count (widest first); returns
 // their number (0 for an unsupported count).
 int i8_tiles(int slices, const I8Tile **out);

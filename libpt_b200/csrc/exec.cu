@@ -11,14 +11,16 @@
 namespace ptb {
 
 bool GemmGroup::operator<(const GemmGroup &o) const {
-  return std::tie(kind, bm, slices, tile.bn, tile.kc) <
-         std::tie(o.kind, o.bm, o.slices, o.tile.bn, o.tile.kc);
+  return std::tie(kind, bm, slices, tile.bn, tile.kc, tile.pair, tile.ts) <
+         std::tie(o.kind, o.bm, o.slices, o.tile.bn, o.tile.kc, o.tile.pair,
+                  o.tile.ts);
 }
 
 std::string GemmGroup::name() const {
   return std::to_string(kind) + "/" + std::to_string(bm) + "/" +
          std::to_string(slices) + "/" + std::to_string(tile.bn) + "/" +
-         std::to_string(tile.kc);
+         std::to_string(tile.kc) + (tile.pair ? "/pair" : "") +
+         (tile.ts ? "/ts" : "");
 }
 
 int GroupMaps::add(const CUtensorMap *d, const CUtensorMap *h, int n) {

@@ -166,16 +166,17 @@ int i8_map_a(CUtensorMap *m, const signed char *p, int64_t K, int64_t R,
     set_error("cuTensorMapEncodeTiled unavailable");
     return LIBPT_ERR_CUDA;
   }
-  const int64_t kpi = i8_kpad(K), nk = kpi / 32, npq = Q * P;
-  cuuint64_t dims[5] = {32, (cuuint64_t)R, (cuuint64_t)nk, (cuuint64_t)npq,
+  constexpr int W = I8_KCHUNK;
+  const int64_t kpi = i8_kpad(K), nk = kpi / W, npq = Q * P;
+  cuuint64_t dims[5] = {W, (cuuint64_t)R, (cuuint64_t)nk, (cuuint64_t)npq,
                         (cuuint64_t)(2 * S)};
-  cuuint64_t str[4] = {32, (cuuint64_t)(R * 32), (cuuint64_t)(R * kpi),
+  cuuint64_t str[4] = {W, (cuuint64_t)(R * W), (cuuint64_t)(R * kpi),
                        (cuuint64_t)(npq * R * kpi)};
-  cuuint32_t box[5] = {32, (cuuint32_t)TC_BM, 1, 1, 1};
+  cuuint32_t box[5] = {W, (cuuint32_t)TC_BM, 1, 1, 1};
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, (void *)p, dims, str,
                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled (INT8 A view) failed: " +
@@ -193,16 +194,17 @@ int i8_map_b(CUtensorMap *m, const signed char *p, int64_t K, int64_t N,
     set_error("cuTensorMapEncodeTiled unavailable");
     return LIBPT_ERR_CUDA;
   }
-  const int64_t kpi = i8_kpad(K), nk = kpi / 32;
-  cuuint64_t dims[5] = {32, (cuuint64_t)N, (cuuint64_t)nk, (cuuint64_t)P,
+  constexpr int W = I8_KCHUNK;
+  const int64_t kpi = i8_kpad(K), nk = kpi / W;
+  cuuint64_t dims[5] = {W, (cuuint64_t)N, (cuuint64_t)nk, (cuuint64_t)P,
                         (cuuint64_t)S};
-  cuuint64_t str[4] = {32, (cuuint64_t)(N * 32), (cuuint64_t)(N * kpi),
+  cuuint64_t str[4] = {W, (cuuint64_t)(N * W), (cuuint64_t)(N * kpi),
                        (cuuint64_t)(P * N * kpi)};
-  cuuint32_t box[5] = {32, (cuuint32_t)bn, 1, 1, 1};
+  cuuint32_t box[5] = {W, (cuuint32_t)bn, 1, 1, 1};
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 5, (void *)p, dims, str,
                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled (INT8 B view) failed: " +
@@ -969,7 +971,8 @@ int i8_encode(libpt_plan *p, SpinCase &c) {
                        p->slices_store)
             : i8_map_b(&c.tcmaps.m[i], c.i8pl[i], d.K, d.N, d.P,
                        p->slices_store,
-                       p->i8tile.bn);
+                       // a CTA of a pair tile loads half of its columns
+                       p->i8tile.pair ? p->i8tile.bn / 2 : p->i8tile.bn);
     if (r) return r;
   }
   return LIBPT_OK;
@@ -1231,7 +1234,7 @@ int plan_append(libpt_plan *p, const int64_t *ents, size_t n, PlanCursor &cur,
                                                                : c.tcmaps.m;
     const int map0 = r.maps[grp].add(c.d_maps, hmaps, tc ? TC_MAX_MAPS : MAX_MAPS);
     const int bn = tc ? TC_BN : i8 ? p->i8tile.bn : GEMM_BN;
-    const int bmr = (tc || i8) ? TC_BM : c.bm;
+    const int bmr = tc ? TC_BM : i8 ? (p->i8tile.pair ? 2 : 1) * TC_BM : c.bm;
     for (const JobT &jt : c.jobs) {
       GemmJob g;
       memset(&g, 0, sizeof(g));
@@ -1522,7 +1525,8 @@ int autotune(libpt_plan *p) {
       if (!r) r = probe_ms(p, p->cases[big], ents, &ms);
       if (!r && tune_verbose())
         std::fprintf(stderr, "libpt autotune %s: INT8 tile %dx%d, K chunk %d B: %.3f ms\n",
-                     key.c_str(), TC_BM, tiles[t].bn, tiles[t].kc, ms);
+                     key.c_str(), (tiles[t].pair ? 2 : 1) * TC_BM, tiles[t].bn,
+                     tiles[t].kc, ms);
       if (!r && (t == 0 || ms < best_ms)) {
         best = t;
         best_ms = ms;

@@ -154,7 +154,7 @@ struct libpt_plan {
   int dbits = 7;                        // digit base bits of the planes (7, 8)
   bool slices_auto = false;             // choose slices for emu_tol
   double emu_tol = 1e-6;                // |dE| target of the choice (Eh)
-  ptb::I8Tile i8tile{64, 32};           // emulated FP64 tile variant
+  ptb::I8Tile i8tile{64, ptb::I8_KCHUNK, 0, 0};   // emulated FP64 tile variant
   std::vector<std::pair<std::pair<const double *, int>, signed char *>> i8planes;
   std::vector<ptb::Family> fams;
   // kernel timing (libpt_plan_timing): events around each round's GEMMs

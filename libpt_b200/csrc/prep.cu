@@ -295,7 +295,8 @@ __global__ void slice_a_kernel(const double *__restrict__ src, int64_t npq,
       digits7(x, S, d);
       for (int q = 0; q < S; ++q) nd[q] = (signed char)(-d[q]);
     }
-    const int64_t o = pq * R * kpi + ((k >> 5) * R + r) * 32 + (k & 31);
+    const int64_t o = pq * R * kpi + ((k / I8_KCHUNK) * R + r) * I8_KCHUNK +
+                      (k % I8_KCHUNK);
     for (int q = 0; q < S; ++q) {
       out[q * plane + o] = d[q];
       out[(S + q) * plane + o] = nd[q];
@@ -334,7 +335,8 @@ __global__ void slice_b_kernel(const double *__restrict__ src, int K,
         digits8(x, S, d);
       else
         digits7(x, S, d);
-      const int64_t o = p * N * kpi + ((int64_t)(k >> 5) * N + n) * 32 + (k & 31);
+      const int64_t o = p * N * kpi + ((int64_t)(k / I8_KCHUNK) * N + n) *
+                                          I8_KCHUNK + (k % I8_KCHUNK);
       for (int q = 0; q < S; ++q) out[q * plane + o] = d[q];
     }
   }

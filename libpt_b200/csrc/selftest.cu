@@ -216,10 +216,13 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
     }
     const I8Tile tl = tiles[variant];
     if ((r = i8_map_a(&(tcmaps_scratch().m[0]), pa, k, m, 1, 1, S)) ||
-        (r = i8_map_b(&(tcmaps_scratch().m[1]), pb1, k, np, 1, S, tl.bn)) ||
-        (r = i8_map_b(&(tcmaps_scratch().m[2]), pb2, k, np, 1, S, tl.bn)))
+        (r = i8_map_b(&(tcmaps_scratch().m[1]), pb1, k, np, 1, S,
+                      tl.pair ? tl.bn / 2 : tl.bn)) ||
+        (r = i8_map_b(&(tcmaps_scratch().m[2]), pb2, k, np, 1, S,
+                      tl.pair ? tl.bn / 2 : tl.bn)))
       return done(r);
-    job.mtiles = (m + TC_BM - 1) / TC_BM;
+    const int bmr = (tl.pair ? 2 : 1) * TC_BM;
+    job.mtiles = (m + bmr - 1) / bmr;
     job.ntiles_n = (int)((np + tl.bn - 1) / tl.bn);
     job.ea = ea;
     job.eb = eb;

@@ -34,7 +34,8 @@ EMU_BOUND = {s: 2.0 ** (-7 * s + 6) for s in (4, 5, 6, 7)}
 EMU8_BOUND = {s: 2.0 ** (-8 * s + 8) for s in (4, 5, 6)}
 
 
-# every compiled INT8 tile variant (tile width x K chunk) of each slice count
+# every compiled INT8 tile variant (tile width x K chunk; one CTA, a CTA
+# pair, or A read from TMEM) of each slice count
 I8_VARIANTS = {4: 4, 5: 4, 6: 3, 7: 1}
 
 
