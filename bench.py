@@ -93,7 +93,7 @@ PRECISIONS = {"fp64": 0, "tf32x3": 1, "emu64": 2}
 # DRAM bytes (read + write) per reference flop of the contraction kernels,
 # from one ncu capture each of restricted (T) o=2, v=477 (two mixed-spin
 # triples, 9.26e11 flops; profiles/gemm_dmma_rpt_o2_v477_fp64_full.txt and
-# profiles/gemm_i8_rpt_o2_v477_emu64s6_full.txt).  A launch's traffic grows
+# profiles/gemm_i8_rpt_o2_v477_emu64s5_full.txt).  A launch's traffic grows
 # with its triples (each reads its own operand slices and writes its own
 # outputs), so the bench scales these by the flops of its launches.
 DRAM_BYTES_PER_FLOP = {"gemm_dmma_kernel": (7.141e9 + 4.338e9) / 9.26e11,
