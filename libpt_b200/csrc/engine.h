@@ -26,8 +26,10 @@ constexpr int MAX_MAPS = 24;
 
 struct GemmSeg {
   int16_t amap, bmap;   // indices into MapSet
-  int16_t neg, pad_;    // neg != 0: subtract this product (INT8: the index
+  int16_t neg;          // neg != 0: subtract this product (INT8: the index
                         // of the first negated digit plane)
+  int16_t half_last;    // INT8: the last K chunk holds <= 32 bytes of K, so
+                        // its second MMA K step (all zero) is skipped
   int32_t a_q, a_p;     // A-view coordinates of dims 2 and 3
   int32_t b_p;          // B-view coordinate of dim 2
   int32_t ksteps;       // ceil(K_s / GEMM_BK)

@@ -348,7 +348,11 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
       const int nseg = job.nseg;
       for (int s = 0; s < nseg && ok; ++s) {
         const int ksteps = job.seg[s].ksteps;
+        const bool half_last = job.seg[s].half_last != 0;
         for (int ks = 0; ks < ksteps && ok; ++ks) {
+          // K steps of this stage: the zero second half of a short last
+          // chunk is skipped
+          const int nkk = (half_last && ks == ksteps - 1) ? 1 : KS;
           if (!mbar_wait(&full[stage], phase, err)) {
             ok = false;
             break;
@@ -366,6 +370,7 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
           const uint32_t later = (s > 0 || ks > 0) ? 1u : 0u;
 #pragma unroll
           for (int kk = 0; kk < KS; ++kk) {
+            if (kk >= nkk) break;
             if constexpr (TS) {
               // region t & 1 was last read by the MMAs of K step t - 2,
               // whose completion regbar[t & 1] records
@@ -584,6 +589,7 @@ __device__ __forceinline__ void i8_pair_body(const LaunchMaps *pm,
       const int nseg = job.nseg;
       for (int s = 0; s < nseg && ok; ++s) {
         const int ksteps = job.seg[s].ksteps;
+        const bool half_last = job.seg[s].half_last != 0;
         for (int ks = 0; ks < ksteps; ++ks) {
           if (!mbar_wait(&full[stage], phase, err)) {
             ok = false;
@@ -594,8 +600,10 @@ __device__ __forceinline__ void i8_pair_body(const LaunchMaps *pm,
           const uint64_t da0 = kmajor_desc<KB>(sa);   // as in i8_body
           const uint64_t db0 = kmajor_desc<KB>(sa + S * C::A_TILE);
           const uint32_t later = (s > 0 || ks > 0) ? 1u : 0u;
+          const int nkk = (half_last && ks == ksteps - 1) ? 1 : KS;
 #pragma unroll
           for (int kk = 0; kk < KS; ++kk) {
+            if (kk >= nkk) break;
 #pragma unroll
             for (int pa = 0; pa < S; ++pa) {
               const uint64_t da =

@@ -1269,6 +1269,8 @@ int plan_append(libpt_plan *p, const int64_t *ents, size_t n, PlanCursor &cur,
                              tc_kchunk_elems(TC_TF32)
                   : i8 ? (st.k + p->i8tile.kc - 1) / p->i8tile.kc
                        : st.ksteps;
+        gs.half_last = (int16_t)(i8 && st.k % p->i8tile.kc != 0 &&
+                                 st.k % p->i8tile.kc <= 32);
       }
       jobs.push_back(g);
     }

@@ -233,6 +233,7 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
       job.seg[s2].bmap = (int16_t)(1 + s2);
       job.seg[s2].neg = (int16_t)(s2 ? S : 0);   // negated planes from S on
       job.seg[s2].ksteps = (k + kc - 1) / kc;
+      job.seg[s2].half_last = (int16_t)(k % kc != 0 && k % kc <= 32);
     }
     publish(&tcmaps_scratch(), sizeof(TcMapSet));
     launch = [=]() {
