@@ -216,9 +216,9 @@ size_t epi_smem_bytes(bool aab, bool ft);
 // persistent: `grid` CTAs stride over list->nblocks tiles (a fixed grid,
 // for graph replay); otherwise a (max tiles of an item) x (items) grid, one
 // CTA per tile, grid = max tiles and nitems the item count.
-cudaError_t epi_aaa_launch(const EpiList *d_list, bool ft, int grid,
+cudaError_t epi_aaa_launch(const EpiList *d_list, bool ft, bool hasf, int grid,
                            int nitems, bool persistent, cudaStream_t st);
-cudaError_t epi_aab_launch(const EpiList *d_list, bool ft, int grid,
+cudaError_t epi_aab_launch(const EpiList *d_list, bool ft, bool hasf, int grid,
                            int nitems, bool persistent, cudaStream_t st);
 // CTAs the epilogue keeps resident per SM (for persistent grids).
 int epi_blocks_per_sm(bool aab, bool ft);

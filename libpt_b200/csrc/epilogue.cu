@@ -28,6 +28,11 @@ namespace ptb {
 
 namespace {
 
+// CTAs per SM the energy kernels are compiled for (80 registers each): the
+// kernels are latency-bound, and three CTAs of 256 threads keep more loads
+// in flight than two (31 -> 40 % of DRAM peak measured), four spill.
+constexpr int EPI_MINB = 3;
+
 __device__ __forceinline__ int64_t pairidx(int p, int q) {
   return (int64_t)p * (p - 1) / 2 + q;
 }
@@ -82,8 +87,8 @@ __device__ __forceinline__ void load_args(EpiArgs &dst, const EpiArgs *src) {
   __syncthreads();
 }
 
-template <bool FT, bool LOOP>
-__global__ void __launch_bounds__(EPI_THREADS, 3)
+template <bool FT, bool LOOP, bool HASF>
+__global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
     epi_aaa_kernel(const EpiList *__restrict__ list) {
   extern __shared__ double sm[];
   __shared__ EpiArgs p;
@@ -107,7 +112,7 @@ __global__ void __launch_bounds__(EPI_THREADS, 3)
   const int a0 = tl.x, b0 = tl.y, c0 = tl.z;
   const int i = item.i, j = item.j, k = item.k;
   const int v = p.va, o = p.oa;
-  const bool has_f = p.has_f != 0;
+  const bool has_f = HASF && p.has_f != 0;   // HASF false: f_ov is zero
   const int g1l = (int)p.g1_ld_aa, g2l = (int)p.g2_ld_aa;
   const double *base = item.ws;
   const double *T = base + p.offL[0];
@@ -201,8 +206,8 @@ __global__ void __launch_bounds__(EPI_THREADS, 3)
 
 // ---------------------------------------------------------------- aab ----
 
-template <bool FT, bool LOOP>
-__global__ void __launch_bounds__(EPI_THREADS, 3)
+template <bool FT, bool LOOP, bool HASF>
+__global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
     epi_aab_kernel(const EpiList *__restrict__ list) {
   extern __shared__ double sm[];
   __shared__ EpiArgs p;
@@ -236,7 +241,7 @@ __global__ void __launch_bounds__(EPI_THREADS, 3)
   const int ld1 = (int)p.ld[0], r1 = (int)p.rowU1;
   const int g1lab = (int)p.g1_ld_ab, g2lab = (int)p.g2_ld_ab;
   const int g1laa = (int)p.g1_ld_aa, g2laa = (int)p.g2_ld_aa;
-  const bool has_f = p.has_f != 0;
+  const bool has_f = HASF && p.has_f != 0;   // HASF false: f_ov is zero
 
   // stage U2 (both orientations) and P asynchronously; the wait comes after
   // the per-thread operand loads below
@@ -381,50 +386,59 @@ int epi_blocks_per_sm(bool aab, bool ft) {
   cudaError_t e;
   if (aab) {
     if (ft) {
-      set_smem(epi_aab_kernel<true, true>, smem);
+      set_smem(epi_aab_kernel<true, true, true>, smem);
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &n, epi_aab_kernel<true, true>, EPI_THREADS, smem);
+          &n, epi_aab_kernel<true, true, true>, EPI_THREADS, smem);
     } else {
-      set_smem(epi_aab_kernel<false, true>, smem);
+      set_smem(epi_aab_kernel<false, true, true>, smem);
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &n, epi_aab_kernel<false, true>, EPI_THREADS, smem);
+          &n, epi_aab_kernel<false, true, true>, EPI_THREADS, smem);
     }
   } else {
     if (ft) {
-      set_smem(epi_aaa_kernel<true, true>, smem);
+      set_smem(epi_aaa_kernel<true, true, true>, smem);
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &n, epi_aaa_kernel<true, true>, EPI_THREADS, smem);
+          &n, epi_aaa_kernel<true, true, true>, EPI_THREADS, smem);
     } else {
-      set_smem(epi_aaa_kernel<false, true>, smem);
+      set_smem(epi_aaa_kernel<false, true, true>, smem);
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &n, epi_aaa_kernel<false, true>, EPI_THREADS, smem);
+          &n, epi_aaa_kernel<false, true, true>, EPI_THREADS, smem);
     }
   }
   return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
-cudaError_t epi_aaa_launch(const EpiList *d_list, bool ft, int grid,
+// Persistent launches (fixed grids, graph replays) use the general kernels;
+// direct launches whose items all have a zero f_ov (hasf false) use the
+// kernels compiled without the f_ov terms.
+cudaError_t epi_aaa_launch(const EpiList *d_list, bool ft, bool hasf, int grid,
                            int nitems, bool persistent, cudaStream_t st) {
   if (grid <= 0 || nitems <= 0) return cudaSuccess;
   const size_t smem = epi_smem_bytes(false, ft);
   const dim3 g(grid, persistent ? 1 : nitems);
   if (persistent)
-    return ft ? launch_epi(epi_aaa_kernel<true, true>, d_list, smem, g, st)
-              : launch_epi(epi_aaa_kernel<false, true>, d_list, smem, g, st);
-  return ft ? launch_epi(epi_aaa_kernel<true, false>, d_list, smem, g, st)
-            : launch_epi(epi_aaa_kernel<false, false>, d_list, smem, g, st);
+    return ft ? launch_epi(epi_aaa_kernel<true, true, true>, d_list, smem, g, st)
+              : launch_epi(epi_aaa_kernel<false, true, true>, d_list, smem, g, st);
+  if (hasf)
+    return ft ? launch_epi(epi_aaa_kernel<true, false, true>, d_list, smem, g, st)
+              : launch_epi(epi_aaa_kernel<false, false, true>, d_list, smem, g, st);
+  return ft ? launch_epi(epi_aaa_kernel<true, false, false>, d_list, smem, g, st)
+            : launch_epi(epi_aaa_kernel<false, false, false>, d_list, smem, g, st);
 }
 
-cudaError_t epi_aab_launch(const EpiList *d_list, bool ft, int grid,
+cudaError_t epi_aab_launch(const EpiList *d_list, bool ft, bool hasf, int grid,
                            int nitems, bool persistent, cudaStream_t st) {
   if (grid <= 0 || nitems <= 0) return cudaSuccess;
   const size_t smem = epi_smem_bytes(true, ft);
   const dim3 g(grid, persistent ? 1 : nitems);
   if (persistent)
-    return ft ? launch_epi(epi_aab_kernel<true, true>, d_list, smem, g, st)
-              : launch_epi(epi_aab_kernel<false, true>, d_list, smem, g, st);
-  return ft ? launch_epi(epi_aab_kernel<true, false>, d_list, smem, g, st)
-            : launch_epi(epi_aab_kernel<false, false>, d_list, smem, g, st);
+    return ft ? launch_epi(epi_aab_kernel<true, true, true>, d_list, smem, g, st)
+              : launch_epi(epi_aab_kernel<false, true, true>, d_list, smem, g, st);
+  if (hasf)
+    return ft ? launch_epi(epi_aab_kernel<true, false, true>, d_list, smem, g, st)
+              : launch_epi(epi_aab_kernel<false, false, true>, d_list, smem, g, st);
+  return ft ? launch_epi(epi_aab_kernel<true, false, false>, d_list, smem, g, st)
+            : launch_epi(epi_aab_kernel<false, false, false>, d_list, smem, g, st);
 }
 
 cudaError_t reduce_partials_launch(const RedList *d_list, int grid,

@@ -41,6 +41,7 @@ void Round::clear() {
     for (int f = 0; f < 2; ++f) {
       epi[a][f].clear();
       epi_blocks[a][f].clear();
+      epi_hasf[a][f] = false;
     }
   red.clear();
   gemm_flops = 0.0;
@@ -198,8 +199,9 @@ int Executor::launch_all(const std::vector<GemmGroup> &groups,
         nitems = (int)r->epi[a][f].size();
       }
       if (grid <= 0) continue;
-      CK(a ? epi_aab_launch(lst, f, grid, nitems, fixed, st_)
-           : epi_aaa_launch(lst, f, grid, nitems, fixed, st_));
+      const bool hasf = fixed || r->epi_hasf[a][f];
+      CK(a ? epi_aab_launch(lst, f, hasf, grid, nitems, fixed, st_)
+           : epi_aaa_launch(lst, f, hasf, grid, nitems, fixed, st_));
       if (launches) ++*launches;
     }
   {

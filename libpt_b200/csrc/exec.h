@@ -45,6 +45,7 @@ struct Round {
   std::map<GemmGroup, GroupMaps> maps;
   std::vector<EpiItem> epi[2][2];                   // [aab][ft], block_begin unset
   std::vector<int> epi_blocks[2][2];                // blocks of each item
+  bool epi_hasf[2][2] = {};                         // some item's f_ov != 0
   std::vector<RedItem> red;
   double gemm_flops = 0.0;                          // reference flops
   size_t triples = 0;

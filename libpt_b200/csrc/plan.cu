@@ -1284,6 +1284,7 @@ int plan_append(libpt_plan *p, const int64_t *ents, size_t n, PlanCursor &cur,
     e.k = q.w;
     r.epi[c.type][p->ft ? 1 : 0].push_back(e);
     r.epi_blocks[c.type][p->ft ? 1 : 0].push_back(c.ntiles);
+    if (p->has_f) r.epi_hasf[c.type][p->ft ? 1 : 0] = true;
     RedItem red;
     red.partials = e.partials;
     red.dst = p->e_slot + ents[t];
