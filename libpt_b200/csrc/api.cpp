@@ -55,11 +55,12 @@ double host_solve(const char *name, int kind, size_t oa, size_t va, size_t ob,
   libpt_plan *p = nullptr;
   double e = 0.0;
   const double t0 = ptb::wall_seconds();
+  // OVVV copies streamed by occupied index next to the triples that need them
   int r = ptb::plan_create(kind, oa, va, ob, vb, args, dtype,
                            dtype ? mp_precision() : fp64_precision(), true, st,
-                           &p);
+                           &p, nullptr, 0, 0, true);
   const double t1 = ptb::wall_seconds();
-  if (!r) r = ptb::plan_run(p, nullptr, p->queue.size());
+  if (!r) r = ptb::plan_run_streamed(p);
   if (!r) r = ptb::plan_energy(p, nullptr, 0, &e);
   if (!r && ptb::profile_enabled())
     fprintf(stderr,

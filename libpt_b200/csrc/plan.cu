@@ -440,17 +440,19 @@ struct Uploader {
   void *stage[2] = {nullptr, nullptr};    // device staging
   size_t stage_bytes = 0;
   int slot = 0;
+  cudaStream_t s = nullptr;               // copy stream (null: the plan's)
 
   int put(double *dst, const void *src, int64_t rows, int64_t w,
           int64_t dpitch) {
     if (rows <= 0 || dpitch <= 0) return LIBPT_OK;
     const size_t es = fp32 ? 4 : 8;
+    const cudaStream_t cs = s ? s : p->st;
     if (!host) {
       if (w == dpitch && !fp32)
         DEV(cudaMemcpyAsync(dst, src, (size_t)rows * w * 8,
-                            cudaMemcpyDeviceToDevice, p->st));
+                            cudaMemcpyDeviceToDevice, cs));
       else
-        DEV(repack_launch(src, fp32, dst, rows, w, dpitch, p->st));
+        DEV(repack_launch(src, fp32, dst, rows, w, dpitch, cs));
       return LIBPT_OK;
     }
     if (!stage[0]) {
@@ -477,16 +479,16 @@ struct Uploader {
         CK(cudaEventSynchronize(ring.done[slot]));   // its last DMA is done
         par_memcpy(ring.buf[slot], from, bytes);
         CK(cudaMemcpyAsync(dstage, ring.buf[slot], bytes,
-                           cudaMemcpyHostToDevice, p->st));
-        CK(cudaEventRecord(ring.done[slot], p->st));
+                           cudaMemcpyHostToDevice, cs));
+        CK(cudaEventRecord(ring.done[slot], cs));
       } else {
-        CK(cudaMemcpyAsync(dstage, from, bytes, cudaMemcpyHostToDevice, p->st));
+        CK(cudaMemcpyAsync(dstage, from, bytes, cudaMemcpyHostToDevice, cs));
       }
       if (flat)
-        CK(repack_launch(dstage, fp32, dst + x0, 1, nx, nx, p->st));
+        CK(repack_launch(dstage, fp32, dst + x0, 1, nx, nx, cs));
       else
         CK(repack_launch(dstage, fp32, dst + x0 * dpitch, nx, w, dpitch,
-                         p->st));
+                         cs));
       slot ^= 1;
     }
     // the ring's buffers may be reused by the next upload only after these
@@ -553,9 +555,13 @@ int upload_set(libpt_plan *p, Uploader &up, const Sizes &S, OperandSet &set,
     } else {
       if (dalloc(p, (void **)&set.ovvv[b], rows * pad4(w) * 8))
         return LIBPT_ERR_NOMEM;
-      if (int r = up.put(set.ovvv[b], (const char *)ovvv + off_v * es, rows, w,
-                         pad4(w)))
+      if (p->defer_ovvv) {   // restricted: the first index is occupied
+        p->deferred.push_back({set.ovvv[b], (const char *)ovvv + off_v * es,
+                               rows / p->oa, w, pad4(w)});
+      } else if (int r = up.put(set.ovvv[b], (const char *)ovvv + off_v * es,
+                                rows, w, pad4(w))) {
         return r;
+      }
     }
     off_v += S.ovvv(b);
   }
@@ -1458,6 +1464,49 @@ int choose_slices(libpt_plan *p) {
 // The probe's energies are discarded (slots reset afterwards); choices do
 // not change results, only speed (each output element is accumulated in
 // the same order by every variant).
+// Sum over the spin cases of the autotuner's probe work (two timed runs per
+// candidate on up to four triples of each case; emulated FP64: of the case
+// with the most work).
+double probe_flops(const libpt_plan *p, int ntiles) {
+  const bool emu = p->precision == LIBPT_PREC_EMU64;
+  double probe = 0.0;
+  for (const SpinCase &c : p->cases)
+    probe = emu ? std::max(probe, 2.0 * ntiles *
+                                      (double)std::min<int64_t>(c.count, 4) *
+                                      c.flops_per_triple)
+                : probe + 4.0 * (double)std::min<int64_t>(c.count, 4) *
+                              c.flops_per_triple;
+  return probe;
+}
+
+// Whether plan creation will run autotuning probes (which read operands).
+bool tune_would_probe(libpt_plan *p) {
+  if (p->queue.empty() || p->precision == LIBPT_PREC_TF32X3 || g_dry)
+    return false;
+  const bool emu = p->precision == LIBPT_PREC_EMU64;
+  const std::string key = tune_key(p->kind, p->oa, p->va, p->ob, p->vb,
+                                   p->precision, emu ? p->slices : 0, p->dtype);
+  std::vector<int> choice;
+  if (tune_lookup(key, &choice) || !tune_enabled()) return false;
+  const I8Tile *tiles = nullptr;
+  const int ntiles = emu ? i8_tiles(p->slices, &tiles) : 0;
+  return probe_flops(p, ntiles) <=
+         0.05 * plan_flops(p, 0, (int64_t)p->queue.size());
+}
+
+// Makes every deferred OVVV copy now (on the plan's stream).
+int flush_deferred(libpt_plan *p) {
+  Uploader up{p, true, p->dtype == 1};
+  up.stage[0] = p->up_stage[0];
+  up.stage[1] = p->up_stage[1];
+  up.stage_bytes = p->up_stage_bytes;
+  for (const DeferredBlock &d : p->deferred)
+    if (int r = up.put(d.dst, d.src, d.rows_per_index * p->oa, d.w, d.dpitch))
+      return r;
+  p->deferred.clear();
+  return LIBPT_OK;
+}
+
 int autotune(libpt_plan *p) {
   if (p->queue.empty() || p->precision == LIBPT_PREC_TF32X3) return LIBPT_OK;
   const bool emu = p->precision == LIBPT_PREC_EMU64;
@@ -1490,13 +1539,7 @@ int autotune(libpt_plan *p) {
   {
     // a small solve keeps the defaults: its probes (two timed runs per
     // candidate) would cost more than a better tile could save
-    double probe = 0.0;
-    for (const SpinCase &c : p->cases)
-      probe = emu ? std::max(probe, 2.0 * ntiles *
-                                        (double)std::min<int64_t>(c.count, 4) *
-                                        c.flops_per_triple)
-                  : probe + 4.0 * (double)std::min<int64_t>(c.count, 4) *
-                                c.flops_per_triple;
+    const double probe = probe_flops(p, ntiles);
     if (probe > 0.05 * plan_flops(p, 0, (int64_t)p->queue.size())) {
       if (tune_verbose())
         std::fprintf(stderr, "libpt autotune %s: skipped (probes %.3g flops "
@@ -1584,7 +1627,7 @@ int autotune(libpt_plan *p) {
 int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
                 const void *const *args, int dtype, int precision, bool host,
                 cudaStream_t st, libpt_plan **out, void *arena,
-                size_t arena_size, size_t arena_nb) {
+                size_t arena_size, size_t arena_nb, bool stream_ovvv) {
   *out = nullptr;
   if (kind < 0 || kind > 3 || dtype < 0 || dtype > 1 || !args) {
     set_error("libpt_plan_create: bad kind/dtype/args");
@@ -1633,6 +1676,8 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
   p->slices = slices;
   p->slices_store = slices;
   p->slices_auto = auto_slices && precision == LIBPT_PREC_EMU64;
+  p->defer_ovvv = stream_ovvv && host && !unr && oa > 0 && va > 0 &&
+                  precision == LIBPT_PREC_FP64;
   if (const char *t = std::getenv("LIBPT_EMU_TOL")) {
     const double v = std::atof(t);
     if (v > 0) p->emu_tol = v;
@@ -1692,6 +1737,9 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
       if (!r) r = upload_set(p, up, S, p->R, args[3], args[6], args[7]);  // t2, i2, i3
     }
     if (r) break;
+    p->up_stage[0] = up.stage[0];   // for the deferred OVVV copies
+    p->up_stage[1] = up.stage[1];
+    p->up_stage_bytes = up.stage_bytes;
     if (!g_dry && cudaStreamSynchronize(st) != cudaSuccess) {
       set_error(std::string("preparing operands: ") +
                 cudaGetErrorString(cudaGetLastError()));
@@ -1804,6 +1852,9 @@ int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
     cudaStreamSynchronize(st);
     p->prof_prepare = wall_seconds() - t_start - p->prof_upload;
   }
+  // deferred OVVV copies stay deferred only when nothing else in creation
+  // reads them (the autotuner's probes would)
+  if (!r && !p->deferred.empty() && tune_would_probe(p)) r = flush_deferred(p);
   const double t_tune = wall_seconds();
   if (!r && !g_dry && p->slices_auto) r = choose_slices(p);
   if (!r && !g_dry) r = autotune(p);
@@ -1860,6 +1911,11 @@ size_t plan_footprint(int kind, size_t oa, size_t va, size_t ob, size_t vb,
 void plan_destroy(libpt_plan *p) {
   if (!p) return;
   if (p->st) cudaStreamSynchronize(p->st);
+  if (p->st_up) {
+    cudaStreamSynchronize(p->st_up);
+    cudaStreamDestroy(p->st_up);
+  }
+  if (p->ev_up) cudaEventDestroy(p->ev_up);
   p->tm.clear();
   if (p->exec_ready) p->exec.destroy();
   for (void *a : p->allocs) cudaFree(a);
@@ -1877,6 +1933,8 @@ double plan_flops(const libpt_plan *p, int64_t first, int64_t n) {
 }
 
 int plan_run(libpt_plan *p, const int64_t *idx, size_t n) {
+  if (!p->deferred.empty())
+    if (int r = flush_deferred(p)) return r;
   const int64_t total = (int64_t)p->queue.size();
   std::vector<int64_t> ents(n);
   for (size_t x = 0; x < n; ++x) {
@@ -1888,6 +1946,52 @@ int plan_run(libpt_plan *p, const int64_t *idx, size_t n) {
     ents[x] = q;
   }
   return run_entries(p, ents);
+}
+
+int plan_run_streamed(libpt_plan *p) {
+  const size_t total = p->queue.size();
+  if (p->deferred.empty()) return plan_run(p, nullptr, total);
+  if (g_dry) return LIBPT_OK;
+  // triples by the largest occupied index they read (every OVVV row a
+  // triple (i, j, k) reads belongs to i, j or k)
+  const int o = p->oa;
+  std::vector<std::vector<int64_t>> by_index((size_t)o);
+  std::vector<int64_t> all(total);
+  for (size_t q = 0; q < total; ++q) {
+    const int4 t = p->queue[q];
+    by_index[(size_t)std::max(t.y, std::max(t.z, t.w))].push_back((int64_t)q);
+    all[q] = (int64_t)q;
+  }
+  // round resources for the whole queue first: growing them later would
+  // wait for the triples already running
+  if (int r = ensure_capacity(p, all)) return r;
+  if (!p->st_up) {
+    CK(cudaStreamCreateWithFlags(&p->st_up, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&p->ev_up, cudaEventDisableTiming));
+  }
+  Uploader up{p, true, p->dtype == 1};
+  up.stage[0] = p->up_stage[0];
+  up.stage[1] = p->up_stage[1];
+  up.stage_bytes = p->up_stage_bytes;
+  up.s = p->st_up;
+  // the copies start after everything plan creation queued on its stream
+  CK(cudaEventRecord(p->ev_up, p->st));
+  CK(cudaStreamWaitEvent(p->st_up, p->ev_up, 0));
+  const size_t es = p->dtype ? 4 : 8;
+  for (int m = 0; m < o; ++m) {
+    for (const DeferredBlock &d : p->deferred) {
+      const int64_t r0 = (int64_t)m * d.rows_per_index;
+      if (int r = up.put(d.dst + r0 * d.dpitch, d.src + (size_t)(r0 * d.w) * es,
+                         d.rows_per_index, d.w, d.dpitch))
+        return r;
+    }
+    CK(cudaEventRecord(p->ev_up, p->st_up));
+    CK(cudaStreamWaitEvent(p->st, p->ev_up, 0));
+    if (!by_index[(size_t)m].empty())
+      if (int r = run_entries(p, by_index[(size_t)m])) return r;
+  }
+  p->deferred.clear();
+  return LIBPT_OK;
 }
 
 int plan_energy(libpt_plan *p, const int64_t *idx, size_t n, double *e,

@@ -109,6 +109,15 @@ struct SpinCase {
 
 }  // namespace ptb
 
+// A host-array OVVV block whose copy is deferred: a restricted FP64
+// host-array solve streams these by occupied index (rows_per_index rows of
+// w elements each) next to the triples that need them.
+struct DeferredBlock {
+  double *dst;              // padded device block (dpitch per row)
+  const char *src;          // the caller's host array
+  int64_t rows_per_index, w, dpitch;
+};
+
 struct libpt_plan {
   int kind = 0;
   bool unrestricted = false, ft = false;
@@ -116,6 +125,14 @@ struct libpt_plan {
   int dtype = 0, precision = 0;
   cudaStream_t st = nullptr;
   double factor = 1.0;
+  // deferred host OVVV copies (plan_run_streamed), their copy stream, the
+  // event that orders the triples after them, and the upload staging
+  bool defer_ovvv = false;   // record host OVVV copies instead of making them
+  std::vector<DeferredBlock> deferred;
+  cudaStream_t st_up = nullptr;
+  cudaEvent_t ev_up = nullptr;
+  void *up_stage[2] = {nullptr, nullptr};
+  size_t up_stage_bytes = 0;
   std::vector<void *> allocs;
   ptb::OperandSet L, R;
   double *d_ov = nullptr, *ov1 = nullptr, *ov2 = nullptr;
@@ -173,7 +190,8 @@ namespace ptb {
 int plan_create(int kind, size_t oa, size_t va, size_t ob, size_t vb,
                 const void *const *args, int dtype, int precision, bool host,
                 cudaStream_t st, libpt_plan **out, void *arena = nullptr,
-                size_t arena_size = 0, size_t arena_nb = 0);
+                size_t arena_size = 0, size_t arena_nb = 0,
+                bool stream_ovvv = false);
 // Exact device bytes plan_create takes from an arena for these arguments
 // with rounds of up to nb triples (a sizing pass: host logic only, no
 // device work); 0 if the arguments are invalid.
@@ -198,6 +216,10 @@ int dmma_map_a(CUtensorMap *m, const double *p, int64_t K, int64_t R,
 int dmma_map_b(CUtensorMap *m, const double *p, int64_t N, int64_t Nld,
                int64_t K, int64_t P);
 int plan_run(libpt_plan *p, const int64_t *idx, size_t n);
+// The whole queue; with deferred OVVV copies, each occupied index's rows are
+// copied on a second stream while the triples whose indices are all below it
+// run (same energies: each triple writes its own slot).
+int plan_run_streamed(libpt_plan *p);
 // Where the next triple of a plan goes in its round resources, and the end
 // of the region this round may use (negative / zero: the plan's capacity),
 // so two rounds of one plan can be in flight in disjoint halves.
