@@ -38,12 +38,12 @@
 //               per stage
 //   warp 1      TMEM owner and MMA issuer (one thread): S(S+1)/2 products
 //               per K step; tcgen05.commit frees the stage
-//   warps 2-9   epilogue: tcgen05.ld of the S accumulators, combined exactly
+//   warps 2-13  epilogue: tcgen05.ld of the S accumulators, combined exactly
 //               in 64-bit integers into two partial sums, one FP64 rounding,
-//               an exact power-of-two scale, FP64 store.  Two warps per TMEM
-//               lane quarter split the tile's 16-column chunks, so the drain
-//               (during which the single-buffered accumulators hold up the
-//               next tile's MMAs) takes half as long.
+//               an exact power-of-two scale, FP64 store.  Three warps per
+//               TMEM lane quarter split the tile's 16-column chunks, so the
+//               drain (during which the single-buffered accumulators hold up
+//               the next tile's MMAs) is short.
 // All mbarrier waits are bounded; on expiry the kernel records the error,
 // stops issuing, still releases TMEM, and returns.
 #include "common.cuh"
@@ -169,19 +169,24 @@ struct I8Cfg {
   static_assert(ST >= 2, "two pipeline stages at least");
 };
 
-constexpr int I8_THREADS = 320;   // producer, MMA issuer, 8 epilogue warps
-constexpr int I8_EPI_THREADS = 256;
+// Epilogue warps per TMEM lane quarter: each drains every third 16-column
+// chunk of its quarter's rows, so the drain (during which the single-
+// buffered accumulators hold up the next tile's MMAs) takes a third as long
+// as with one warp per quarter.
+constexpr int I8_EPI_GROUPS = 3;
+constexpr int I8_EPI_THREADS = 4 * I8_EPI_GROUPS * 32;
+constexpr int I8_THREADS = 64 + I8_EPI_THREADS;   // producer, MMA, epilogue
 
 // Drains one tile's accumulators (this CTA's 128 rows, rows from m0): the
 // S INT32 sums of each element folded exactly, rounded once, scaled and
-// stored.  Called by the 8 epilogue warps after the tile's accumulators are
+// stored.  Called by the epilogue warps after the tile's accumulators are
 // complete.
 template <int S, int BN>
 __device__ __forceinline__ void i8_drain(const GemmJob &job, int m0, int n0,
                                          uint32_t tmem, int warp, int lane) {
   constexpr int H = (S + 1) / 2;
   const int q = warp & 3;            // TMEM lane quarter of this warp
-  const int half = (warp - 2) >> 2;  // which 16-column chunks it takes
+  const int grp = (warp - 2) >> 2;   // which 16-column chunks it takes
   // digit base 2^b; weights of the two partial sums: hi counts units of
   // acc_{H-1}, lo units of acc_{S-1}
   const int b = job.dbits == 8 ? 8 : 7, g = b == 8 ? 2 : 0;
@@ -195,7 +200,7 @@ __device__ __forceinline__ void i8_drain(const GemmJob &job, int m0, int n0,
   const int erow = rok ? job.ea[row] : 0;
   const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
 #pragma unroll 1
-  for (int c0 = 16 * half; c0 < BN; c0 += 32) {
+  for (int c0 = 16 * grp; c0 < BN; c0 += 16 * I8_EPI_GROUPS) {
     // exact: acc_0..acc_{H-1} and acc_H..acc_{S-1} folded by Horner in base
     // 2^b into 64-bit integers; |acc| < 2^31 and each sum has at most 4
     // terms of base 2^7 or 3 of base 2^8 (8-bit digits only for S <= 6), so

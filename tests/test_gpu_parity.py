@@ -100,6 +100,18 @@ def test_device_twin_equals_host_entry(kind, sz):
     assert e_mp == ffi.solve_host(case, mp=True)
 
 
+@pytest.mark.parametrize("kind,sz,fock", [
+    ("rpt", (2, 9), 0.0), ("rpt", (3, 17), 1e-3), ("rpt", (7, 33), 0.0),
+    ("rft", (2, 8), 1e-3), ("rft", (5, 21), 0.0)])
+def test_streamed_host_upload_equals_device_inputs(kind, sz, fock):
+    """Restricted FP64 host-array solves copy i_ovvv (and i3/i7_ovvv) by
+    occupied index beside the triples that need them: the energy is the
+    device-input energy bitwise, including queues whose first indices own
+    no triple (o = 2, 3) and a nonzero f_ov."""
+    case = synth.make(kind, *sz, seed=31, fock=fock)
+    assert ffi.solve_host(case) == ffi.solve_device(case, to_dev(case))
+
+
 def test_zero_sizes():
     for kind, sz in [("rpt", (0, 5)), ("rpt", (3, 0)), ("rpt", (3, 1)),
                      ("upt", (2, 3, 0, 4)), ("uft", (0, 3, 2, 4))]:
