@@ -264,6 +264,30 @@ def run_cpu(o, v, reps, threads_mode="blas"):
 # ------------------------------------------------------------------ arms
 
 
+def workload_config(args, world):
+    """The `config` both arms report: the sampled o, v workload of one step
+    (restricted queue: C(o,3) same-spin then C(o,2)*o mixed-spin triples;
+    per-triple flops of src/pt.c's dgemm_ calls, as rpt_flops)."""
+    o, v = args.o, float(args.v)
+    naaa = o * (o - 1) * (o - 2) // 6
+    n = naaa + o * (o - 1) // 2 * o
+    stride = max(1, args.stride // world)
+    sample = np.arange(0, n, stride, dtype=np.int64)
+    nsame = int((sample < naaa).sum())
+    f_aaa = 3 * v**3 * (v - 1) + 6 * o * v**3
+    f_aab = 6 * v**4 + 2 * v**3 * (v - 1) + 10 * o * v**3
+    return dict(
+        workload=f"rpt o={args.o} v={args.v}: every {stride}th triple of the "
+                 f"{n}-entry queue per step ({len(sample)} triples, {nsame} "
+                 "same-spin)",
+        precision=args.precision.split(",")[0],
+        parallelism="1 GPU" if world == 1 else
+        f"triples sharded x{world} (entry q on rank q % {world}), one "
+        "energy-slot all-reduce per step",
+        l2="inputs (74 GB) larger than L2; no flush needed",
+        flops_per_step=nsame * f_aaa + (len(sample) - nsame) * f_aab)
+
+
 def run_reference(args, d):
     """Reference arm: the reference's own CPU implementation (oracle/_ref:
     src/pt.c + OpenBLAS, OpenMP) on full solves of o=2, v=477."""
@@ -288,14 +312,13 @@ def run_reference(args, d):
         warmup=args.warmup, ms_per_step=res["seconds"] * 1e3,
         higher_is_better=True, scaling="weak", vs_baseline=None,
         dtype="f64", data="synthetic", impl="reference",
-        config=dict(workload=f"libpt_rpt full solves o={args.cpu_o} "
-                             f"v={args.v} (sample of the o=45 v=477 "
-                             "workload: same virtual space)",
-                    o=args.cpu_o, v=args.v),
+        config=workload_config(args, args.gpus),
         cpu_baseline=dict(value=val, unit="TFLOP/s", cores=res["cores"],
                           kind="reference",
-                          sample=f"libpt_rpt o={args.cpu_o} v={args.v} "
-                                 f"(OpenMP 1 thread, OpenBLAS "
+                          sample=f"bounded sample of the workload: full "
+                                 f"libpt_rpt solves of o={args.cpu_o} "
+                                 f"v={args.v} (the same virtual space; "
+                                 f"OpenMP 1 thread, OpenBLAS "
                                  f"{res['cores']} threads)"),
         e2e=dict(value=val, unit="TFLOP/s", h2d_bytes_per_step=0,
                  d2h_bytes_per_step=0),
@@ -458,17 +481,7 @@ def run_ours(args, d):
             warmup=args.warmup, ms_per_step=secs_max / args.steps * 1e3,
             higher_is_better=True, scaling="weak", vs_baseline=None,
             dtype="f64", data="synthetic",
-            config=dict(
-                workload=f"rpt o={args.o} v={args.v}: every "
-                         f"{max(1, args.stride // d.world)}th triple of the "
-                         f"{plan_n}-entry queue per step ({R0['nsample']} "
-                         f"triples, {R0['nsame']} same-spin)",
-                precision=head,
-                parallelism="1 GPU" if d.world == 1 else
-                f"triples sharded x{d.world} (entry q on rank q % "
-                f"{d.world}), one energy-slot all-reduce per step",
-                l2="inputs (74 GB) larger than L2; no flush needed",
-                flops_per_step=R0["flops_all"]),
+            config=workload_config(args, d.world),
             projected_solve_seconds=flops_full / (value * 1e12),
             roofline=dict(bound="tensor", achieved=ach, peak=peak64,
                           unit="TFLOP/s", frac=ach / peak64,
