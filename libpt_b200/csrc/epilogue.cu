@@ -229,8 +229,16 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
   if (!LOOP && local >= item.nblk) return;
   load_args(p, item.args);
   const int npairs = p.ntiles / p.ctiles;   // tiles: c block major
-  const int4 tl = p.tiles[local % npairs];
-  const int a0 = tl.x, b0 = tl.y, c0 = (local / npairs) * EPI_C;
+  // the (a, b) tiles are the triangle a0 = 8t, b0 = 8u, u <= t, in row
+  // order (the last row may stop at u = t - 1); tile L sits in row
+  // t = floor((sqrt(8L + 1) - 1) / 2), computed here instead of loaded from
+  // the case's tile table, so the data loads need one dependent load less
+  const int L = local % npairs;
+  int t = (int)((sqrtf(8.0f * (float)L + 1.0f) - 1.0f) * 0.5f);
+  while ((t + 1) * (t + 2) / 2 <= L) ++t;
+  while (t * (t + 1) / 2 > L) --t;
+  const int a0 = EPI_A * t, b0 = EPI_B * (L - t * (t + 1) / 2);
+  const int c0 = (local / npairs) * EPI_C;
   const int i = item.i, j = item.j, k = item.k;
   const int oa = p.oa, va = p.va, ob = p.ob, vb = p.vb;
   const double *base = item.ws;
