@@ -180,10 +180,13 @@ constexpr int I8_THREADS = 64 + I8_EPI_THREADS;   // producer, MMA, epilogue
 // Drains one tile's accumulators (this CTA's 128 rows, rows from m0): the
 // S INT32 sums of each element folded exactly, rounded once, scaled and
 // stored.  Called by the epilogue warps after the tile's accumulators are
-// complete.
-template <int S, int BN>
+// complete.  `release` runs once per thread as soon as the thread's last
+// TMEM loads have completed (before that chunk's stores), so the next
+// tile's MMAs may start overwriting the accumulators while it stores.
+template <int S, int BN, typename Release>
 __device__ __forceinline__ void i8_drain(const GemmJob &job, int m0, int n0,
-                                         uint32_t tmem, int warp, int lane) {
+                                         uint32_t tmem, int warp, int lane,
+                                         Release release) {
   constexpr int H = (S + 1) / 2;
   const int q = warp & 3;            // TMEM lane quarter of this warp
   const int grp = (warp - 2) >> 2;   // which 16-column chunks it takes
@@ -199,8 +202,10 @@ __device__ __forceinline__ void i8_drain(const GemmJob &job, int m0, int n0,
   double *const orow = job.out + (int64_t)(rok ? row : 0) * job.ldc;
   const int erow = rok ? job.ea[row] : 0;
   const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
+  constexpr int STEP = 16 * I8_EPI_GROUPS;
+  if (16 * grp >= BN) release();   // no chunk for this warp
 #pragma unroll 1
-  for (int c0 = 16 * grp; c0 < BN; c0 += 16 * I8_EPI_GROUPS) {
+  for (int c0 = 16 * grp; c0 < BN; c0 += STEP) {
     // exact: acc_0..acc_{H-1} and acc_H..acc_{S-1} folded by Horner in base
     // 2^b into 64-bit integers; |acc| < 2^31 and each sum has at most 4
     // terms of base 2^7 or 3 of base 2^8 (8-bit digits only for S <= 6), so
@@ -232,6 +237,7 @@ __device__ __forceinline__ void i8_drain(const GemmJob &job, int m0, int n0,
         lo[x] = l;
       }
     }
+    if (c0 + STEP >= BN) release();   // warp-uniform: the last chunk
     if (rok && n0 + c0 < N) {
       // the chunk's 16 column exponents in one aligned 16-byte load (the
       // exponent arrays carry 16 bytes of padding past their N entries)
@@ -440,9 +446,10 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
       if (!mbar_wait(accfull, (uint32_t)(it & 1), err)) break;
       tc_fence_after();
       i8_drain<S, BN>(job, (local % job.mtiles) * BM,
-                      (local / job.mtiles) * BN, tmem, warp, lane);
-      tc_fence_before();
-      mbar_arrive(accempty);
+                      (local / job.mtiles) * BN, tmem, warp, lane, [&] {
+                        tc_fence_before();
+                        mbar_arrive(accempty);
+                      });
     }
   }
   // all roles done: release TMEM
@@ -644,10 +651,11 @@ __device__ __forceinline__ void i8_pair_body(const LaunchMaps *pm,
       if (!mbar_wait(accfull, (uint32_t)(it & 1), err)) break;
       tc_fence_after();
       i8_drain<S, BN>(job, (local % job.mtiles) * 2 * BM + (int)rank * BM,
-                      (local / job.mtiles) * BN, tmem, warp, lane);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive_cluster(accempty_lead);
+                      (local / job.mtiles) * BN, tmem, warp, lane, [&] {
+                        tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive_cluster(accempty_lead);
+                      });
     }
   }
   // all roles of both CTAs done: release TMEM
