@@ -22,7 +22,12 @@ Lines printed (rank 0, one JSON line):
              tensor peak (cuBLAS DGEMM measured here, MEASURED_PEAKS.json
              having no FP64 figure)
   cpu_baseline  the reference library (oracle/_ref, OpenMP + OpenBLAS) timed
-             on the host cores on a full solve of o=2, v=477 (rank 0, N=1)
+             on the host cores on a full solve of o=2, v=477 (rank 0, N=1),
+             with the o=45 solve's time extrapolated from that rate
+  precision_table  |dE| of every precision form: restricted o=8, v=64
+             against the reference run with one thread (plus the
+             reference's own 1-vs-all-threads spread), then unrestricted (T)
+             and (fT) against the FP64 path
 --impl reference prints the reference's own CPU implementation on the same
 sample workload (o=2, v=477 full solves), with all host threads.
 
@@ -247,7 +252,10 @@ def run_cpu(o, v, reps, threads_mode="blas"):
     env = dict(os.environ)
     if threads_mode == "blas":    # few triples: give the cores to BLAS
         env.update(OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS=str(n))
-    else:
+    elif threads_mode == "single":  # one thread: a fixed summation order
+        n = 1
+        env.update(OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1")
+    else:                         # OpenMP over triples (src/pt.c:227-230)
         env.update(OMP_NUM_THREADS=str(n), OPENBLAS_NUM_THREADS="1")
     r = subprocess.run([sys.executable, os.path.abspath(__file__),
                         "--cpu-worker", "--cpu-o", str(o), "--v", str(v),
@@ -259,6 +267,17 @@ def run_cpu(o, v, reps, threads_mode="blas"):
     out["cores"] = n
     out["threads"] = threads_mode
     return out
+
+
+def extrapolation(args, tflops):
+    """The full o, v solve on the host cores, extrapolated from the measured
+    sample rate (the workload's queue flops over that rate: a solve too large
+    for the host's memory and hours of CPU time is not run in full)."""
+    return dict(
+        extrapolated_solve_seconds=rpt_flops(args.o, args.v) / (tflops * 1e12),
+        extrapolation=f"extrapolated: rpt o={args.o} v={args.v} reference "
+                      f"flops ({rpt_flops(args.o, args.v):.4g}) over the rate "
+                      f"measured on the o={args.cpu_o} v={args.v} sample")
 
 
 # ------------------------------------------------------------------ arms
@@ -319,7 +338,8 @@ def run_reference(args, d):
                                  f"libpt_rpt solves of o={args.cpu_o} "
                                  f"v={args.v} (the same virtual space; "
                                  f"OpenMP 1 thread, OpenBLAS "
-                                 f"{res['cores']} threads)"),
+                                 f"{res['cores']} threads)",
+                          **extrapolation(args, val)),
         e2e=dict(value=val, unit="TFLOP/s", h2d_bytes_per_step=0,
                  d2h_bytes_per_step=0),
         wall_seconds=wall)
@@ -458,17 +478,25 @@ def run_ours(args, d):
     accuracy = None
     if not args.no_accuracy:
         accuracy = run_accuracy(args, torch)
+        if d.rank == 0:
+            try:
+                accuracy.insert(0, run_accuracy_reference(torch))
+            except Exception as ex:   # report, do not fail the bench
+                accuracy.insert(0, dict(kind="rpt", sizes=[8, 64],
+                                        failed=f"{ex}"[:300]))
 
     cpu = None
     if not args.no_cpu and d.world == 1 and d.rank == 0:
         try:
             r = run_cpu(args.cpu_o, args.v, 1)
-            cpu = dict(value=r["flops"] / r["seconds"] / 1e12, unit="TFLOP/s",
+            rate = r["flops"] / r["seconds"] / 1e12
+            cpu = dict(value=rate, unit="TFLOP/s",
                        cores=r["cores"], kind="reference",
                        sample=f"reference libpt_rpt (oracle/_ref) full solve "
                               f"o={args.cpu_o} v={args.v}, "
                               f"{r['seconds']:.1f} s; OpenMP 1 thread, "
-                              f"OpenBLAS {r['cores']} threads")
+                              f"OpenBLAS {r['cores']} threads",
+                       **extrapolation(args, rate))
         except Exception as ex:   # report, do not fail the bench
             cpu = dict(value=None, unit="TFLOP/s", cores=os.cpu_count(),
                        kind="reference", sample=f"failed: {ex}"[:300])
@@ -621,6 +649,54 @@ def run_serving(args, torch, gpu_id):
                  "arrivals (service times measured)"))
 
 
+def precision_forms(ffi):
+    """(name, precision word, FP32 inputs) of every form the tables report."""
+    forms = [("fp64", ffi.PREC_FP64, False)]
+    forms += [(f"emu64_s{s}", ffi.PREC_EMU64 | (s << 8), False)
+              for s in (4, 5, 6, 7)]
+    forms += [("emu64_auto", ffi.PREC_EMU64, False)]   # S chosen for 1 uEh
+    forms += [("tf32x3", ffi.PREC_TF32X3, True)]
+    return forms
+
+
+def run_accuracy_reference(torch, o=8, v=64, seed=7):
+    """Restricted (T) o=8, v=64 (host inputs, seed 7) in every precision form
+    against the reference build run with one OpenMP and one BLAS thread (a
+    fixed summation order), plus the reference's own spread between that
+    run and one with OpenMP over triples on all host cores (src/pt.c:227-230,
+    a dynamic schedule whose summation order varies)."""
+    from libpt_b200 import ffi, synth
+    from oracle import oracle
+    row = dict(kind="rpt", sizes=[o, v], seed=seed)
+    if not os.path.exists(oracle.reference_path()):
+        row["unavailable"] = "oracle/_ref/libpt_ref.so was not built"
+        return row
+    r1 = run_cpu(o, v, 1, "single")
+    rn = run_cpu(o, v, 1, "omp")
+    e_ref = r1["energy"]
+    row.update(reference_energy=e_ref,
+               reference="oracle/_ref, OpenMP 1 thread, OpenBLAS 1 thread",
+               reference_thread_spread_Eh=abs(rn["energy"] - e_ref),
+               reference_threads=rn["cores"])
+    case = synth.rpt_case(o, v, seed=seed)
+    dev = {n: torch.as_tensor(case[n]).to(device="cuda", dtype=torch.float64)
+           for n in ffi.PT_ARGS}
+    res = {}
+    for name, prec, mp in precision_forms(ffi):
+        src = {k: x.float() for k, x in dev.items()} if mp else dev
+        p = ffi.Plan(case, src, mp=mp, precision=prec)
+        try:
+            p.run()
+            e = p.energy()
+            sl = p.slices or None
+        finally:
+            p.close()
+        res[name] = dict(energy=e, slices=sl, dE_uEh=abs(e - e_ref) * 1e6,
+                         dE_rel=abs(e - e_ref) / abs(e_ref) if e_ref else None)
+    row["forms"] = res
+    return row
+
+
 def run_accuracy(args, torch):
     """Full solves of unrestricted (T) oa=20 va=180 ob=18 vb=182 and
     unrestricted (fT) o=15 v=150 (spin blocks 15/150 each), inputs generated
@@ -633,11 +709,7 @@ def run_accuracy(args, torch):
     cases = [("upt", (20, 180, 18, 182)), ("uft", (15, 150, 15, 150))]
     if args.accuracy_rft:
         cases.append(("rft", (30, 300)))
-    forms = [("fp64", ffi.PREC_FP64, False)]
-    forms += [(f"emu64_s{s}", ffi.PREC_EMU64 | (s << 8), False)
-              for s in (4, 5, 6, 7)]
-    forms += [("emu64_auto", ffi.PREC_EMU64, False)]   # S chosen for 1 uEh
-    forms += [("tf32x3", ffi.PREC_TF32X3, True)]
+    forms = precision_forms(ffi)
     rows = []
     for kind, sz in cases:
         meta, tens = synth.case_device(kind, *sz, seed=7)
