@@ -22,14 +22,20 @@ Lines printed (rank 0, one JSON line):
              tensor peak (cuBLAS DGEMM measured here, MEASURED_PEAKS.json
              having no FP64 figure)
   cpu_baseline  the reference library (oracle/_ref, OpenMP + OpenBLAS) timed
-             on the host cores on a full solve of o=2, v=477 (rank 0, N=1),
-             with the o=45 solve's time extrapolated from that rate
-  precision_table  |dE| of every precision form: restricted o=8, v=64
-             against the reference run with one thread (plus the
-             reference's own 1-vs-all-threads spread), then unrestricted (T)
-             and (fT) against the FP64 path
---impl reference prints the reference's own CPU implementation on the same
-sample workload (o=2, v=477 full solves), with all host threads.
+             on the host cores (rank 0, N=1) on one same-spin and one
+             mixed-spin triple at v=477, with the o=45 solve's time
+             extrapolated from the two kinds' rates
+  serving    the served stream (continuous batching, pt_serve.h) at 20, 50
+             and 100 requests/s beside one-at-a-time FP64 solves
+  precision_table  |dE| of every precision form against the reference
+             build's FP64 energy of the same inputs (and the reference's own
+             FP32 *_mp beside the FP32 forms): restricted (T) o=8 v=64,
+             unrestricted (T) 20/180/18/182, unrestricted (fT) 15/150 per
+             spin; restricted (fT) o=30 v=300 against the FP64 path
+--impl reference prints the reference's own CPU implementation on its
+per-kind sample of the workload's triples, with all host threads.
+--full-solve runs one full o=45 v=477 solve through libpt_rpt in FP64 and
+in emulated FP64 instead (about 16 minutes).
 
 Multi-GPU (torchrun): the ranks shard one solve the way the reference's MPI
 build does (src/pt.c:213, 474-477): identical inputs on every GPU, a sample
@@ -56,7 +62,7 @@ if ROOT not in sys.path:
 O_FULL, V_FULL = 45, 477      # the workload (restricted, all-electron)
 STRIDE = 211                  # triples-queue sampling stride of one step
 O_E2E = 4                     # full solves through the host API
-O_CPU = 2                     # full solves of the reference on the host
+O_CPU = 0                     # the reference's host sample (0: per kind)
 
 
 def parse():
@@ -73,23 +79,35 @@ def parse():
     ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--cpu-o", type=int, default=O_CPU)
     ap.add_argument("--cpu-reps", type=int, default=1)
+    ap.add_argument("--cpu-warmup", type=int, default=0,
+                    help=argparse.SUPPRESS)
     ap.add_argument("--precision", default="fp64,emu64",
                     help="comma list of fp64, emu64, tf32x3; the first is "
                          "the headline value")
-    ap.add_argument("--serve-slices", type=int, default=6,
-                    help="digit slices of the served stream's emulated half")
+    ap.add_argument("--serve-slices", type=int, default=0,
+                    help="digit slices of the served stream's emulated half "
+                         "(0: chosen per solve for 1 uEh)")
     ap.add_argument("--slices", type=int, default=0,
                     help="emulated FP64 digit slices (4..7; 0: chosen by the "
                          "plan for LIBPT_EMU_TOL, default 1e-6 Eh)")
-    ap.add_argument("--serve-requests", type=int, default=40,
-                    help="requests of the served stream (0: skip)")
-    ap.add_argument("--serve-rate", type=float, default=20.0,
-                    help="Poisson arrival rate of the served stream (req/s)")
+    ap.add_argument("--serve-requests", type=int, default=30,
+                    help="requests of the served stream at each rate "
+                         "(0: skip)")
+    ap.add_argument("--serve-rates", default="20,50,100",
+                    help="Poisson arrival rates of the served stream (req/s)")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the precision table (unrestricted (T) and (fT))")
-    ap.add_argument("--accuracy-rft", action="store_true",
-                    help="add restricted (fT) o=30 v=300 to the table (~2 min)")
+    ap.add_argument("--no-rft", action="store_true",
+                    help="leave restricted (fT) o=30 v=300 out of the "
+                         "precision table (~2 min)")
+    ap.add_argument("--cpu-seed", type=int, default=7, help=argparse.SUPPRESS)
+    ap.add_argument("--full-solve", action="store_true",
+                    help="instead of the sampled steps: one full o, v "
+                         "restricted (T) solve through libpt_rpt (host "
+                         "arrays) in FP64, then in emulated FP64 with the "
+                         "slice count chosen for 1 uEh (~16 min at o=45, "
+                         "v=477); prints one JSON line")
     return ap.parse_args()
 
 
@@ -230,24 +248,66 @@ def fp64_peak_tflops(torch):
     return best
 
 
+def aaa_flops(o, v):
+    """Reference dgemm_ flops of one same-spin triple (src/pt.c:49, 110):
+    3 v^3 (v-1) + 6 o v^3."""
+    v = float(v)
+    return 3 * v**3 * (v - 1) + 6 * o * v**3
+
+
+def aab_flops(oa, va, ob, vb):
+    """Reference dgemm_ flops of one mixed-spin triple (src/pt.c:65, 81, 97,
+    126, 142, 158): 2 va^3 vb + 4 va^2 vb^2 + 2 vb va^2 (va-1)
+    + 6 va^2 vb oa + 4 va^2 vb ob."""
+    va, vb = float(va), float(vb)
+    return (2 * va**3 * vb + 4 * va**2 * vb**2 + 2 * vb * va**2 * (va - 1)
+            + 6 * va**2 * vb * oa + 4 * va**2 * vb * ob)
+
+
 def cpu_worker(args):
-    """Time the reference library (oracle/_ref) on full rpt solves of
-    (cpu-o, v); prints one JSON line.  Run in a subprocess so that the
-    OpenMP/OpenBLAS thread counts apply from library load."""
+    """Time the reference library (oracle/_ref); prints one JSON line.  Run
+    in a subprocess so that the OpenMP/OpenBLAS thread counts apply from
+    library load.  --cpu-o > 0: full libpt_rpt solves of (cpu-o, v).
+    --cpu-o 0: the per-kind sample -- one same-spin triple (libpt_upt with
+    oa=3, ob=0: its only triple) and one mixed-spin triple (libpt_upt with
+    oa=2, ob=1, vb=va: its only triple), each timed on its own, per rep."""
     from libpt_b200 import synth
     from oracle import oracle
-    case = synth.rpt_case(args.cpu_o, args.v, seed=7)
     ref = oracle.reference()
     oracle.solve(ref, synth.rpt_case(2, 24, seed=1))   # load + thread spin-up
-    t0 = time.perf_counter()
+    if args.cpu_o > 0:
+        case = synth.rpt_case(args.cpu_o, args.v, seed=args.cpu_seed)
+        t0 = time.perf_counter()
+        for _ in range(args.cpu_reps):
+            e = oracle.solve(ref, case)
+        dt = (time.perf_counter() - t0) / args.cpu_reps
+        print(json.dumps(dict(seconds=dt, flops=rpt_flops(args.cpu_o, args.v),
+                              energy=e)))
+        return
+    v = args.v
+    c_aaa = synth.upt_case(3, v, 0, 1, seed=args.cpu_seed)
+    c_aab = synth.upt_case(2, v, 1, v, seed=args.cpu_seed)
+    for _ in range(args.cpu_warmup):
+        oracle.solve(ref, c_aaa)
+        oracle.solve(ref, c_aab)
+    t_aaa = t_aab = 0.0
     for _ in range(args.cpu_reps):
-        e = oracle.solve(ref, case)
-    dt = (time.perf_counter() - t0) / args.cpu_reps
-    print(json.dumps(dict(seconds=dt, flops=rpt_flops(args.cpu_o, args.v),
-                          energy=e)))
+        t0 = time.perf_counter()
+        e_aaa = oracle.solve(ref, c_aaa)
+        t1 = time.perf_counter()
+        e_aab = oracle.solve(ref, c_aab)
+        t_aaa += t1 - t0
+        t_aab += time.perf_counter() - t1
+    n = args.cpu_reps
+    print(json.dumps(dict(v=v, seconds_aaa=t_aaa / n, seconds_aab=t_aab / n,
+                          flops_aaa=aaa_flops(3, v),
+                          flops_aab=aab_flops(2, v, 1, v),
+                          seconds=(t_aaa + t_aab) / n,
+                          flops=aaa_flops(3, v) + aab_flops(2, v, 1, v),
+                          energy=e_aaa + e_aab)))
 
 
-def run_cpu(o, v, reps, threads_mode="blas"):
+def run_cpu(o, v, reps, threads_mode="blas", seed=7, warmup=0):
     n = os.cpu_count() or 1
     env = dict(os.environ)
     if threads_mode == "blas":    # few triples: give the cores to BLAS
@@ -259,7 +319,8 @@ def run_cpu(o, v, reps, threads_mode="blas"):
         env.update(OMP_NUM_THREADS=str(n), OPENBLAS_NUM_THREADS="1")
     r = subprocess.run([sys.executable, os.path.abspath(__file__),
                         "--cpu-worker", "--cpu-o", str(o), "--v", str(v),
-                        "--cpu-reps", str(reps)],
+                        "--cpu-reps", str(reps), "--cpu-seed", str(seed),
+                        "--cpu-warmup", str(warmup)],
                        env=env, capture_output=True, text=True, timeout=1800)
     if r.returncode != 0:
         raise RuntimeError(r.stderr[-2000:])
@@ -269,15 +330,28 @@ def run_cpu(o, v, reps, threads_mode="blas"):
     return out
 
 
-def extrapolation(args, tflops):
-    """The full o, v solve on the host cores, extrapolated from the measured
-    sample rate (the workload's queue flops over that rate: a solve too large
-    for the host's memory and hours of CPU time is not run in full)."""
+def extrapolation(args, r):
+    """The full o, v restricted solve on the host cores, extrapolated from
+    the per-kind sample (a solve too large for the host's memory and days of
+    CPU time is not run in full): C(o,3) same-spin and C(o,2) o mixed-spin
+    triples, each at the flop rate measured for its kind on the sample (the
+    per-triple flops grow with o through the OOVO contractions; the rate of
+    each kind is taken to stay the same)."""
+    o, v = args.o, args.v
+    n_aaa = o * (o - 1) * (o - 2) // 6
+    n_aab = o * (o - 1) // 2 * o
+    rate_aaa = r["flops_aaa"] / r["seconds_aaa"]
+    rate_aab = r["flops_aab"] / r["seconds_aab"]
+    secs = (n_aaa * aaa_flops(o, v) / rate_aaa
+            + n_aab * aab_flops(o, v, o, v) / rate_aab)
     return dict(
-        extrapolated_solve_seconds=rpt_flops(args.o, args.v) / (tflops * 1e12),
-        extrapolation=f"extrapolated: rpt o={args.o} v={args.v} reference "
-                      f"flops ({rpt_flops(args.o, args.v):.4g}) over the rate "
-                      f"measured on the o={args.cpu_o} v={args.v} sample")
+        extrapolated_solve_seconds=secs,
+        rate_same_spin_tflops=rate_aaa / 1e12,
+        rate_mixed_spin_tflops=rate_aab / 1e12,
+        extrapolation=f"extrapolated: rpt o={o} v={v}, {n_aaa} same-spin "
+                      f"triples at the same-spin rate and {n_aab} mixed-spin "
+                      "triples at the mixed-spin rate measured on the "
+                      f"v={v} sample")
 
 
 # ------------------------------------------------------------------ arms
@@ -307,9 +381,23 @@ def workload_config(args, world):
         flops_per_step=nsame * f_aaa + (len(sample) - nsame) * f_aab)
 
 
+def sample_description(r):
+    v = r["v"]
+    return (f"reference libpt_upt (oracle/_ref) per step: one same-spin "
+            f"triple (oa=3, ob=0, va={v}; {r['seconds_aaa']:.1f} s) and one "
+            f"mixed-spin triple (oa=2, ob=1, va=vb={v}; "
+            f"{r['seconds_aab']:.1f} s), the two kinds of triple of the "
+            f"restricted v={v} queues; OpenMP 1 thread, OpenBLAS "
+            f"{r['cores']} threads (a step of two triples leaves OpenMP over "
+            "triples nothing to spread)")
+
+
 def run_reference(args, d):
     """Reference arm: the reference's own CPU implementation (oracle/_ref:
-    src/pt.c + OpenBLAS, OpenMP) on full solves of o=2, v=477."""
+    src/pt.c + OpenBLAS, OpenMP) on the per-kind sample of the workload's
+    triples -- one same-spin and one mixed-spin triple at v=477 per step --
+    with W untimed warm-up steps; the o=45 solve's time is extrapolated
+    from the two kinds' rates."""
     if d.rank != 0:
         return
     from oracle import oracle
@@ -318,10 +406,8 @@ def run_reference(args, d):
             "oracle/_ref/libpt_ref.so was not built (needs the reference "
             "source tree at build time)"))))
         return
-    if args.warmup > 0:
-        run_cpu(args.cpu_o, args.v, 1)
     t0 = time.perf_counter()
-    res = run_cpu(args.cpu_o, args.v, max(args.steps, 1))
+    res = run_cpu(0, args.v, max(args.steps, 1), warmup=args.warmup)
     wall = time.perf_counter() - t0
     val = res["flops"] / res["seconds"] / 1e12
     line = dict(
@@ -331,15 +417,16 @@ def run_reference(args, d):
         warmup=args.warmup, ms_per_step=res["seconds"] * 1e3,
         higher_is_better=True, scaling="weak", vs_baseline=None,
         dtype="f64", data="synthetic", impl="reference",
-        config=workload_config(args, args.gpus),
+        config=dict(workload="per step one same-spin and one mixed-spin "
+                             f"triple at v={args.v} (the two kinds of "
+                             f"triple of the rpt o={args.o} v={args.v} "
+                             "queue), reference CPU library",
+                    precision="fp64",
+                    parallelism=f"host CPU, {res['cores']} threads",
+                    flops_per_step=res["flops"]),
         cpu_baseline=dict(value=val, unit="TFLOP/s", cores=res["cores"],
-                          kind="reference",
-                          sample=f"bounded sample of the workload: full "
-                                 f"libpt_rpt solves of o={args.cpu_o} "
-                                 f"v={args.v} (the same virtual space; "
-                                 f"OpenMP 1 thread, OpenBLAS "
-                                 f"{res['cores']} threads)",
-                          **extrapolation(args, val)),
+                          kind="reference", sample=sample_description(res),
+                          **extrapolation(args, res)),
         e2e=dict(value=val, unit="TFLOP/s", h2d_bytes_per_step=0,
                  d2h_bytes_per_step=0),
         wall_seconds=wall)
@@ -478,25 +565,16 @@ def run_ours(args, d):
     accuracy = None
     if not args.no_accuracy:
         accuracy = run_accuracy(args, torch)
-        if d.rank == 0:
-            try:
-                accuracy.insert(0, run_accuracy_reference(torch))
-            except Exception as ex:   # report, do not fail the bench
-                accuracy.insert(0, dict(kind="rpt", sizes=[8, 64],
-                                        failed=f"{ex}"[:300]))
 
     cpu = None
     if not args.no_cpu and d.world == 1 and d.rank == 0:
         try:
-            r = run_cpu(args.cpu_o, args.v, 1)
+            r = run_cpu(0, args.v, 1)
             rate = r["flops"] / r["seconds"] / 1e12
             cpu = dict(value=rate, unit="TFLOP/s",
                        cores=r["cores"], kind="reference",
-                       sample=f"reference libpt_rpt (oracle/_ref) full solve "
-                              f"o={args.cpu_o} v={args.v}, "
-                              f"{r['seconds']:.1f} s; OpenMP 1 thread, "
-                              f"OpenBLAS {r['cores']} threads",
-                       **extrapolation(args, rate))
+                       sample=sample_description(r),
+                       **extrapolation(args, r))
         except Exception as ex:   # report, do not fail the bench
             cpu = dict(value=None, unit="TFLOP/s", cores=os.cpu_count(),
                        kind="reference", sample=f"failed: {ex}"[:300])
@@ -574,178 +652,349 @@ def percentile(x, q):
     return float(np.percentile(np.asarray(x), q)) if len(x) else None
 
 
+PHASES = ("admission_wait_s", "prepare_s", "first_round_wait_s", "running_s")
+
+
 def run_serving(args, torch, gpu_id):
-    """Served stream through the continuous-batching server (pt_serve.h):
-    each request's inputs are generated on the device when it arrives and
-    submitted; latency runs from submission to its energy.  Beside it, the
-    same requests as one-at-a-time FP64 solves (libpt plan per request,
-    FIFO at the same arrival times, queueing computed from the measured
-    service times)."""
+    """Served stream through the continuous-batching server (pt_serve.h) at
+    each arrival rate of --serve-rates.  The same requests at every rate
+    (serve_stream: sizes, seeds and the order of arrivals fixed, arrival
+    times scaled by 1/rate); their inputs are prepared in host memory before
+    the stream starts (generated on the device, copied out) and submitted as
+    host arrays at their arrival times, as requests arriving from outside
+    would be; latency runs from submission to the energy.  Per rate:
+    solves/s, p50 / p99 latency, where the p99 request's time went
+    (admission wait, preparation, wait for its first round, running; the
+    server's libpt_server_solve_times) and the mean of each phase, rounds
+    and graph-replayed rounds.  Beside it, the same requests as
+    one-at-a-time FP64 solves through libpt_rpt (host arrays), FIFO at the
+    same arrivals: service times measured once, queueing computed per
+    rate."""
     from libpt_b200 import ffi, synth
-    reqs = serve_stream(args.serve_requests, args.serve_rate, seed=4)
+    rates = [float(x) for x in args.serve_rates.split(",") if x]
+    reqs = serve_stream(args.serve_requests, 1.0, seed=4)   # unit rate
     emu = ffi.PREC_EMU64 | (args.serve_slices << 8)
+    t_prep = time.perf_counter()
+    cases = []
+    for r in reqs:
+        meta, tens = synth.rpt_case_device(r["o"], r["v"], seed=r["seed"])
+        case = dict(meta)
+        case.update({k: t.cpu().numpy() for k, t in tens.items()})
+        del tens
+        cases.append(case)
+    torch.cuda.empty_cache()
+    t_prep = time.perf_counter() - t_prep
+    host_gb = sum(sum(a.nbytes for k, a in c.items()
+                      if isinstance(a, np.ndarray)) for c in cases) / 2**30
     budget = int(args.serve_budget_gb * (1 << 30))
-    free = torch.cuda.mem_get_info()[0]
-    # room beside the pool for arriving requests' inputs until admission
-    budget = min(budget, int(free - (24 << 30)))
-    flops = 0.0
-    srv = ffi.Server(mem_budget=budget)
-    clocks = Clocks(gpu_id)
-    clocks.start()
-    t0 = time.perf_counter()
-    tickets = []
-    for r in reqs:
-        while time.perf_counter() - t0 < r["arrival"]:
-            time.sleep(0.0005)
-        srv.release_inputs()            # inputs already resident in the pool
-        meta, tens = synth.rpt_case_device(r["o"], r["v"], seed=r["seed"])
-        torch.cuda.synchronize()
-        tickets.append(srv.submit(meta, tensors=tens,
-                                  precision=emu if r["emu"] else 0))
-        del tens
-        flops += rpt_flops(r["o"], r["v"])
-    lat, energies = [], []
-    for tk in tickets:
-        e, l = srv.wait(tk)
-        lat.append(l)
-        energies.append(e)
-    wall = time.perf_counter() - t0
-    clk = clocks.stop()
-    st = srv.stats()
-    srv.close()
-    torch.cuda.empty_cache()
-    # one-at-a-time FP64 solves of the same requests
+    budget = min(budget, int(torch.cuda.mem_get_info()[0] - (8 << 30)))
+    flops = sum(rpt_flops(r["o"], r["v"]) for r in reqs)
+    n = len(reqs)
+    # one-at-a-time FP64 service times (libpt_rpt, uploads included)
     service = []
-    for r in reqs:
-        meta, tens = synth.rpt_case_device(r["o"], r["v"], seed=r["seed"])
-        torch.cuda.synchronize()
+    for case in cases:
         a = time.perf_counter()
-        p = ffi.Plan(meta, tens)
-        p.run()
-        p.energy()
-        p.close()
+        ffi.solve_host(case)
         service.append(time.perf_counter() - a)
-        del tens
-    torch.cuda.empty_cache()
-    done, blat = 0.0, []
-    for r, sv in zip(reqs, service):
-        done = max(done, r["arrival"]) + sv
-        blat.append(done - r["arrival"])
+    per_rate = []
+    for rate in rates:
+        srv = ffi.Server(mem_budget=budget)
+        clocks = Clocks(gpu_id)
+        clocks.start()
+        t0 = time.perf_counter()
+        tickets = []
+        for r, case in zip(reqs, cases):
+            while time.perf_counter() - t0 < r["arrival"] / rate:
+                time.sleep(0.0005)
+            tickets.append(srv.submit(case, precision=emu if r["emu"] else 0))
+        lat, phases = [], []
+        for tk in tickets:
+            lat.append(srv.wait(tk)[1])
+            phases.append(srv.times(tk))
+        wall = time.perf_counter() - t0
+        clk = clocks.stop()
+        st = srv.stats()
+        srv.close()
+        done, blat = 0.0, []
+        for r, sv in zip(reqs, service):
+            a = r["arrival"] / rate
+            done = max(done, a) + sv
+            blat.append(done - a)
+        i99 = int(np.argsort(lat)[min(n - 1, int(np.ceil(0.99 * n)) - 1)])
+        ph = np.asarray(phases)
+        span = reqs[-1]["arrival"] / rate
+        per_rate.append(dict(
+            rate=rate,
+            offered_tflops=flops / span / 1e12 if span > 0 else None,
+            solves_per_s=n / wall, tflops=flops / wall / 1e12,
+            p50_s=percentile(lat, 50), p99_s=percentile(lat, 99),
+            p99_request=dict(o=reqs[i99]["o"], v=reqs[i99]["v"],
+                             emulated=reqs[i99]["emu"], latency_s=lat[i99],
+                             **dict(zip(PHASES, map(float, ph[i99])))),
+            mean_phases_s=dict(zip(PHASES, map(float, ph.mean(axis=0)))),
+            rounds=st["rounds"], graph_rounds=st["graph_rounds"],
+            max_resident=st["max_resident"],
+            peak_pool_gb=st["peak_bytes_in_use"] / 2**30, clocks=clk,
+            one_at_a_time_fp64=dict(solves_per_s=n / done,
+                                    p50_s=percentile(blat, 50),
+                                    p99_s=percentile(blat, 99))))
     return dict(
-        workload=f"{len(reqs)} restricted (T) requests, o~U{{4..24}}, "
-                 f"v=round(o*U[6,12]), Poisson {args.serve_rate:g} req/s, "
-                 f"half FP64 / half emulated FP64 ({args.serve_slices} slices), "
-                 "inputs generated on the device at arrival",
-        solves_per_s=len(reqs) / wall, p50_s=percentile(lat, 50),
-        p99_s=percentile(lat, 99), tflops=flops / wall / 1e12,
-        rounds=st["rounds"], graph_rounds=st["graph_rounds"],
-        max_resident=st["max_resident"],
-        peak_pool_gb=st["peak_bytes_in_use"] / 2**30,
-        pool_gb=st["pool_bytes"] / 2**30, clocks=clk,
-        one_at_a_time_fp64=dict(
-            solves_per_s=len(reqs) / done, p50_s=percentile(blat, 50),
-            p99_s=percentile(blat, 99),
-            note="sequential FP64 plan per request, FIFO queue at the same "
-                 "arrivals (service times measured)"))
+        workload=f"{n} restricted (T) requests per rate, o~U{{4..24}}, "
+                 "v=round(o*U[6,12]), Poisson arrivals, half FP64 / half "
+                 "emulated FP64 (slices "
+                 + ("chosen for 1 uEh" if args.serve_slices == 0 else
+                    f"fixed at {args.serve_slices}")
+                 + f"), host inputs ({host_gb:.1f} GiB, prepared in "
+                 f"{t_prep:.0f} s before the streams)",
+        flops=flops, pool_gb=budget / 2**30,
+        sustainable_solves_per_s=max(r["solves_per_s"] for r in per_rate),
+        sustainable_note="the highest throughput measured: every rate "
+                         "offers more work than the GPU completes, so each "
+                         "stream runs at capacity and its latency is "
+                         "queueing",
+        one_at_a_time_fp64_solves_per_s=n / sum(service),
+        one_at_a_time_note="sequential libpt_rpt (FP64, host arrays) per "
+                           "request; FIFO queueing at each rate's arrivals "
+                           "computed from the measured service times",
+        per_rate=per_rate)
 
 
-def precision_forms(ffi):
-    """(name, precision word, FP32 inputs) of every form the tables report."""
+def precision_forms(ffi, slices=(4, 5, 6)):
+    """(name, precision word, FP32 inputs) of every form the tables report:
+    FP64 DMMA; emulated FP64 with fixed and chosen (1 uEh) slice counts; on
+    the FP32-rounded inputs the FP32 tensor-core form (the *_mp default),
+    the FP64 engine (the floor every FP32-input method shares) and 3xTF32."""
     forms = [("fp64", ffi.PREC_FP64, False)]
     forms += [(f"emu64_s{s}", ffi.PREC_EMU64 | (s << 8), False)
-              for s in (4, 5, 6, 7)]
+              for s in slices]
     forms += [("emu64_auto", ffi.PREC_EMU64, False)]   # S chosen for 1 uEh
-    forms += [("tf32x3", ffi.PREC_TF32X3, True)]
+    forms += [("fp32_tc", ffi.PREC_FP32, True),
+              ("fp64_on_fp32_inputs", ffi.PREC_FP64, True),
+              ("tf32x3", ffi.PREC_TF32X3, True)]
     return forms
 
 
-def run_accuracy_reference(torch, o=8, v=64, seed=7):
-    """Restricted (T) o=8, v=64 (host inputs, seed 7) in every precision form
-    against the reference build run with one OpenMP and one BLAS thread (a
-    fixed summation order), plus the reference's own spread between that
-    run and one with OpenMP over triples on all host cores (src/pt.c:227-230,
-    a dynamic schedule whose summation order varies)."""
-    from libpt_b200 import ffi, synth
-    from oracle import oracle
-    row = dict(kind="rpt", sizes=[o, v], seed=seed)
-    if not os.path.exists(oracle.reference_path()):
-        row["unavailable"] = "oracle/_ref/libpt_ref.so was not built"
-        return row
-    r1 = run_cpu(o, v, 1, "single")
-    rn = run_cpu(o, v, 1, "omp")
-    e_ref = r1["energy"]
-    row.update(reference_energy=e_ref,
-               reference="oracle/_ref, OpenMP 1 thread, OpenBLAS 1 thread",
-               reference_thread_spread_Eh=abs(rn["energy"] - e_ref),
-               reference_threads=rn["cores"])
-    case = synth.rpt_case(o, v, seed=seed)
-    dev = {n: torch.as_tensor(case[n]).to(device="cuda", dtype=torch.float64)
-           for n in ffi.PT_ARGS}
-    res = {}
-    for name, prec, mp in precision_forms(ffi):
-        src = {k: x.float() for k, x in dev.items()} if mp else dev
+# Cases of the precision table with reference energies (FP64 and the
+# reference's FP32 *_mp) computed by the reference build on the same
+# host-generated inputs (tests/golden/make_reference_energies.py writes
+# tests/golden/reference_energies.json; the reference does not travel).
+PRECISION_CASES = [("rpt_8_64", "rpt", (8, 64), 7),
+                   ("upt_20_180_18_182", "upt", (20, 180, 18, 182), 7),
+                   ("uft_15_150", "uft", (15, 150, 15, 150), 7)]
+
+
+def reference_energies():
+    path = os.path.join(ROOT, "tests", "golden", "reference_energies.json")
+    if not os.path.exists(path):
+        return {}
+    with open(path) as fp:
+        return json.load(fp)
+
+
+def input_sha256(case):
+    import hashlib
+    from libpt_b200 import ffi
+    h = hashlib.sha256()
+    for n in ffi.args_of(case["kind"]):
+        h.update(np.ascontiguousarray(case[n], dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def run_forms(torch, case, dev64, forms):
+    """Plan + full solve of one case in each form: energy, seconds (solve,
+    plan creation apart), TFLOP/s of the reference's flops, slices."""
+    from libpt_b200 import ffi
+    dev32 = {k: x.float() for k, x in dev64.items()}
+    res, fl = {}, None
+    for name, prec, mp in forms:
+        src = dev32 if mp else dev64
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         p = ffi.Plan(case, src, mp=mp, precision=prec)
-        try:
-            p.run()
-            e = p.energy()
-            sl = p.slices or None
-        finally:
-            p.close()
-        res[name] = dict(energy=e, slices=sl, dE_uEh=abs(e - e_ref) * 1e6,
-                         dE_rel=abs(e - e_ref) / abs(e_ref) if e_ref else None)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        p.run()
+        e = p.energy()
+        t2 = time.perf_counter()
+        fl = p.flops()
+        res[name] = dict(energy=e, seconds=t2 - t1, plan_seconds=t1 - t0,
+                         tflops=fl / (t2 - t1) / 1e12, slices=p.slices or None)
+        p.close()
+    del dev32
+    for r in res.values():
+        r["speedup_vs_fp64"] = res["fp64"]["seconds"] / r["seconds"]
+    return res, fl
+
+
+def run_precision_case(torch, name, kind, sz, seed, refs, forms):
+    """One row of the precision table: every form on host-generated inputs
+    (synth.make, the seed of the reference energies), |dE| against the
+    reference build's FP64 energy, beside the reference's own FP32 *_mp.
+    For the FP32-input forms the arithmetic part is also given against the
+    FP64 engine on the same FP32-rounded inputs (the floor)."""
+    from libpt_b200 import synth
+    case = synth.make(kind, *sz, seed=seed)
+    row = dict(kind=kind, sizes=list(sz), seed=seed)
+    ref = refs.get(name)
+    if ref is None:
+        row["reference"] = "no reference energy committed for this case"
+    elif ref["input_sha256"] != input_sha256(case):
+        row["reference"] = "inputs differ from the reference run's (sha256)"
+        ref = None
+    dev = {n: torch.as_tensor(np.ascontiguousarray(case[n])).to(
+        device="cuda", dtype=torch.float64) for n in args_of_kind(kind)}
+    del case
+    res, fl = run_forms(torch, dict(kind=kind, oa=sz[0], va=sz[1],
+                                    ob=sz[2] if len(sz) > 2 else sz[0],
+                                    vb=sz[3] if len(sz) > 2 else sz[1]),
+                        dev, forms)
+    del dev
+    torch.cuda.empty_cache()
+    row["flops"] = fl
+    floor = res["fp64_on_fp32_inputs"]["energy"]
+    if ref is not None:
+        e_ref, e_mp = ref["fp64"]["energy"], ref["fp32_mp"]["energy"]
+        row["reference"] = dict(
+            energy=e_ref, seconds=ref["fp64"]["seconds"],
+            cores=ref["cores"], threads=ref["threads"],
+            source="oracle/_ref (the reference built from its sources), "
+                   "tests/golden/reference_energies.json")
+        row["reference_fp32_mp"] = dict(
+            energy=e_mp, seconds=ref["fp32_mp"]["seconds"],
+            dE_uEh=abs(e_mp - e_ref) * 1e6,
+            dE_rel=abs(e_mp - e_ref) / abs(e_ref),
+            arith_dE_rel=abs(e_mp - floor) / abs(e_ref))
+    else:
+        e_ref = res["fp64"]["energy"]
+        row["dE_against"] = "the FP64 path"
+    for n, r in res.items():
+        r["dE_uEh"] = abs(r["energy"] - e_ref) * 1e6
+        r["dE_rel"] = abs(r["energy"] - e_ref) / abs(e_ref) if e_ref else None
+        if n in ("fp32_tc", "tf32x3"):
+            r["arith_dE_rel"] = abs(r["energy"] - floor) / abs(e_ref)
     row["forms"] = res
     return row
 
 
+def args_of_kind(kind):
+    from libpt_b200 import ffi
+    return ffi.args_of(kind)
+
+
 def run_accuracy(args, torch):
-    """Full solves of unrestricted (T) oa=20 va=180 ob=18 vb=182 and
-    unrestricted (fT) o=15 v=150 (spin blocks 15/150 each), inputs generated
-    on the device, in every precision form: FP64 (DMMA), emulated FP64 with
-    4-7 INT8 slices, and 3xTF32 on the FP32 inputs.  |dE| against the FP64
-    path (the FP64 path matches the reference FP64 build to <= 1e-12 |E| in
-    the parity tests; the CPU reference itself would need ~10 min here).
-    Seconds exclude plan creation (reported apart)."""
+    """The precision table.  Restricted (T) o=8 v=64, unrestricted (T)
+    oa=20 va=180 ob=18 vb=182 and unrestricted (fT) o=15 v=150 per spin, on
+    host-generated inputs, every form against the reference build's FP64
+    and FP32 (*_mp) energies of the same inputs (committed, with the input
+    digest); restricted (fT) o=30 v=300 (device-generated; the reference
+    would need hours) against the FP64 path.  The o=8 v=64 row also carries
+    the reference's own 1-thread vs all-threads spread, measured here."""
     from libpt_b200 import ffi, synth
-    cases = [("upt", (20, 180, 18, 182)), ("uft", (15, 150, 15, 150))]
-    if args.accuracy_rft:
-        cases.append(("rft", (30, 300)))
-    forms = precision_forms(ffi)
+    refs = reference_energies()
     rows = []
-    for kind, sz in cases:
-        meta, tens = synth.case_device(kind, *sz, seed=7)
-        res = {}
-        for name, prec, mp in forms:
-            src = {k: x.float() for k, x in tens.items()} if mp else tens
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            p = ffi.Plan(meta, src, mp=mp, precision=prec)
-            torch.cuda.synchronize()
-            t1 = time.perf_counter()
-            p.run()
-            e = p.energy()
-            t2 = time.perf_counter()
-            fl = p.flops()
-            sl = p.slices or None
-            p.close()
-            del src
-            res[name] = dict(seconds=t2 - t1, plan_seconds=t1 - t0,
-                             tflops=fl / (t2 - t1) / 1e12, energy=e,
-                             slices=sl)
-        e64 = res["fp64"]["energy"]
-        for name, r in res.items():
-            r["dE_uEh"] = abs(r["energy"] - e64) * 1e6
-            r["dE_rel"] = abs(r["energy"] - e64) / abs(e64) if e64 else None
-            r["speedup_vs_fp64"] = res["fp64"]["seconds"] / r["seconds"]
-        rows.append(dict(kind=kind, sizes=list(sz), flops=fl, forms=res))
+    for name, kind, sz, seed in PRECISION_CASES:
+        forms = precision_forms(ffi, (4, 5, 6, 7) if kind == "rpt" else
+                                (4, 5, 6))
+        row = run_precision_case(torch, name, kind, sz, seed, refs, forms)
+        if name == "rpt_8_64":
+            try:
+                r1 = run_cpu(sz[0], sz[1], 1, "single", seed=seed)
+                rn = run_cpu(sz[0], sz[1], 1, "omp", seed=seed)
+                row["reference_thread_spread_Eh"] = abs(rn["energy"] -
+                                                        r1["energy"])
+                row["reference_threads"] = rn["cores"]
+            except Exception as ex:   # report, do not fail the bench
+                row["reference_thread_spread_Eh"] = f"failed: {ex}"[:200]
+        rows.append(row)
+    if not args.no_rft:
+        meta, tens = synth.case_device("rft", 30, 300, seed=7)
+        forms = [f for f in precision_forms(ffi, ())
+                 if f[0] in ("fp64", "emu64_auto", "fp32_tc")]
+        res, fl = run_forms(torch, meta, tens, forms)
         del tens
         torch.cuda.empty_cache()
+        e64 = res["fp64"]["energy"]
+        for r in res.values():
+            r["dE_uEh"] = abs(r["energy"] - e64) * 1e6
+            r["dE_rel"] = abs(r["energy"] - e64) / abs(e64)
+        rows.append(dict(kind="rft", sizes=[30, 300], flops=fl,
+                         dE_against="the FP64 path (pinned at this size by "
+                                    "the rft = uft(closed shell) identity, "
+                                    "tests/test_gpu_slow.py)",
+                         forms=res))
     return rows
+
+
+def run_full_solve(args):
+    """One full restricted (T) solve of the workload through the
+    reference-facing host entry point libpt_rpt, first FP64 (DMMA), then
+    emulated FP64 (LIBPT_FP64_PRECISION=emu64: slice count chosen by the plan
+    for |dE| <= LIBPT_EMU_TOL, default 1e-6 Eh).  The inputs are generated on
+    the device (the bench's generator and seed), copied to host arrays and
+    released on the device, so each timed call includes the upload of every
+    pt.h array.  Wall-clock seconds of each call, TFLOP/s of the reference's
+    flops, and the full-solve |dE| of the emulated form against FP64."""
+    import torch
+    from libpt_b200 import ffi, synth
+    torch.cuda.set_device(0)
+    props = torch.cuda.get_device_properties(0)
+    gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else "0"
+    meta, tens = synth.rpt_case_device(args.o, args.v, seed=1000)
+    nbytes = sum(t.numel() * 8 for t in tens.values())
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = None
+    out = dict(metric="full restricted (T) solve through libpt_rpt (host "
+                      "arrays)", workload=f"rpt o={args.o} v={args.v}, "
+                      "synthetic (device generator, seed 1000)",
+               flops=rpt_flops(args.o, args.v), h2d_bytes=nbytes,
+               host_bytes_available=avail)
+    if avail is not None and avail < 1.15 * nbytes:
+        out["unavailable"] = (f"host RAM: {avail / 2**30:.0f} GiB available, "
+                              f"{nbytes / 2**30:.0f} GiB of inputs")
+        print(json.dumps(out))
+        return
+    case = dict(meta)
+    for k in list(tens):
+        case[k] = tens[k].cpu().numpy()
+        del tens[k]
+    del tens
+    torch.cuda.empty_cache()
+    runs = {}
+    for name, env in (("fp64", None), ("emu64", "emu64")):
+        if env:
+            os.environ["LIBPT_FP64_PRECISION"] = env
+        else:
+            os.environ.pop("LIBPT_FP64_PRECISION", None)
+        clocks = Clocks(gpu_id)
+        clocks.start()
+        t0 = time.perf_counter()
+        e = ffi.solve_host(case)
+        dt = time.perf_counter() - t0
+        runs[name] = dict(seconds=dt, tflops=out["flops"] / dt / 1e12,
+                          energy=e, clocks=clocks.stop())
+        print(f"full solve {name}: {dt:.1f} s, E = {e!r}", file=sys.stderr,
+              flush=True)
+    os.environ.pop("LIBPT_FP64_PRECISION", None)
+    e64 = runs["fp64"]["energy"]
+    for r in runs.values():
+        r["dE_uEh"] = abs(r["energy"] - e64) * 1e6
+        r["dE_rel"] = abs(r["energy"] - e64) / abs(e64)
+    runs["emu64"]["speedup_vs_fp64"] = (runs["fp64"]["seconds"] /
+                                        runs["emu64"]["seconds"])
+    out["runs"] = runs
+    print(json.dumps(out))
 
 
 def main():
     args = parse()
     if args.cpu_worker:
         cpu_worker(args)
+        return
+    if args.full_solve:
+        run_full_solve(args)
         return
     d = Dist()
     if args.impl == "reference":

@@ -91,6 +91,7 @@ double libpt_uft_mp(size_t oa, size_t va, size_t ob, size_t vb,
 #define LIBPT_ERR_CUDA       3   /* a CUDA runtime/driver call failed       */
 #define LIBPT_ERR_TIMEOUT    4   /* a device-side wait ran out of its limit */
 #define LIBPT_ERR_UNSUPPORTED 5  /* option not available on this device     */
+#define LIBPT_ERR_CANCELLED  6   /* a served solve was cancelled (pt_serve.h) */
 
 /* Text of the last error on the calling thread ("" if none). */
 const char *libpt_last_error(void);
@@ -99,27 +100,49 @@ const char *libpt_last_error(void);
 
 #define LIBPT_PREC_FP64   0   /* FP64 DMMA tensor-core contractions          */
 #define LIBPT_PREC_TF32X3 1   /* 3xTF32 on tcgen05 tensor cores (hi*hi +
-                                 hi*lo + lo*hi, FP32 accumulation in TMEM):
-                                 ~1e-5 relative per contraction element; the
-                                 *_mp entry points use it when the environment
-                                 sets LIBPT_MP_PRECISION=tf32x3 (otherwise
-                                 they evaluate FP32 inputs in FP64)          */
+                                 hi*lo + lo*hi, FP32 accumulation in TMEM).
+                                 The tensor cores' FP32 accumulation
+                                 truncates, a bias that adds up coherently
+                                 over a solve: ~2e-6 |E| on synthetic
+                                 inputs, 1e3-1e4 times the reference *_mp's
+                                 own arithmetic error.  Opt-in only
+                                 (LIBPT_MP_PRECISION=tf32x3).                 */
 
 #define LIBPT_PREC_EMU64  2   /* emulated FP64: Ozaki-style split of FP64
-                                 operands into S signed 7-bit digit planes
-                                 (power-of-two scale per row / column), exact
-                                 INT32 accumulation of the S(S+1)/2 leading
-                                 digit products on tcgen05 INT8 tensor cores.
+                                 operands into S signed digit planes (8-bit
+                                 balanced digits, or 7-bit ones where the
+                                 INT32 bound needs them; power-of-two scale
+                                 per row / column), exact INT32 accumulation
+                                 of the S(S+1)/2 leading digit products on
+                                 tcgen05 INT8 tensor cores.
                                  LIBPT_PREC_EMU64 | (S << 8) fixes S in
                                  [4, 7]; S = 0 lets the plan choose the
-                                 smallest S whose error bound, estimated on a
-                                 sample of triples against 7 slices, is under
-                                 LIBPT_EMU_TOL / 2 (environment, Eh; default
-                                 1e-6, i.e. 1 uEh).  The FP64 entry points
-                                 (libpt_rpt ... and their _dev twins) use it
-                                 when the environment sets
-                                 LIBPT_FP64_PRECISION=emu64 (S chosen) or
-                                 emu64:S; otherwise they run FP64 DMMA      */
+                                 smallest S whose error, estimated on a
+                                 sample of triples against the most stored
+                                 planes, is under LIBPT_EMU_TOL / 2
+                                 (environment, Eh; default 1e-6, i.e.
+                                 1 uEh).  The FP64 entry points (libpt_rpt
+                                 ... and their _dev twins) use it when the
+                                 environment sets LIBPT_FP64_PRECISION=emu64
+                                 (S chosen) or emu64:S; otherwise they run
+                                 FP64 DMMA                                   */
+
+#define LIBPT_PREC_FP32   3   /* the FP32 tensor-core form, default of the
+                                 *_mp entry points: FP32 inputs split into 5
+                                 INT8 digit planes (39-bit significands,
+                                 beyond FP32's 24), digits rounded to
+                                 nearest, exact INT32 accumulation on tcgen05
+                                 INT8 tensor cores, energy terms in FP64.
+                                 Unlike FP32 accumulation (rounded or
+                                 truncated), its per-element error is both
+                                 unbiased and far below FP32 rounding, so
+                                 the result carries the rounding of the FP32
+                                 inputs themselves plus an arithmetic error
+                                 under 1 % of the reference's sgemm_ path's
+                                 (src/ptmp.c:28-38).  LIBPT_MP_PRECISION=fp64
+                                 evaluates the FP32 inputs with the FP64
+                                 engine instead, =tf32x3 with 3xTF32.  A
+                                 plan reports 5 slices.                      */
 
 /* Built-in self-test of a contraction kernel: C = A B1 - A B2 on random
  * m x k and k x n operands, against an FP64 reference computed on the device;
@@ -146,6 +169,17 @@ int libpt_selftest_variants(int precision);
  * NULL).  The job does 4*m*n*k flops.  No counterpart in the reference. */
 int libpt_kernel_bench(int precision, int m, int n, int k, int reps,
                        double *ms, double *rel_err);
+/* Failure-detection self-test of the device-side bounded waits: a
+ * producer / consumer kernel passes `stages` hand-offs through a ring of
+ * mbarriers (as the contraction kernels' pipelines do), but its producer
+ * stops after `arrive` of them.  Each wait is limited to limit_ms
+ * (0 < limit_ms <= 2000; the kernels' own limit is 2 s): a missing hand-off
+ * makes the consumer's wait run out, the kernel records the timeout in its
+ * error word and returns, and the call returns LIBPT_ERR_TIMEOUT -- the
+ * status a solve reports when one of its kernels' waits runs out; the
+ * device stays usable.  *seen = hand-offs the consumer received.  No
+ * counterpart in the reference. */
+int libpt_selftest_wait(int stages, int arrive, double limit_ms, int *seen);
 
 /* ---- device-pointer twins ----------------------------------------------
  * Same arguments as the reference entry points, but every tensor is a
@@ -198,11 +232,16 @@ int libpt_uft_mp_dev(size_t oa, size_t va, size_t ob, size_t vb,
  * synchronize the device.  Same arguments and result as libpt_rpt_dev (FP64
  * device tensors in pt.h layout on the current device), but it allocates
  * nothing: all scratch lives in one static device array of
- * LIBPT_STATIC_SCRATCH_BYTES, which every GPU that loads the library keeps
- * until the process exits.  Systems whose scratch does not fit are rejected
- * with LIBPT_ERR_ARG before any work is queued (o = 8, v = 64 fits).
- * The first call on a device looks up the array's device address (a one-time
- * set-up per device); make that first call before any stream capture.
+ * LIBPT_STATIC_SCRATCH_BYTES, which every GPU that loads the library's
+ * device code keeps until the process exits.  Systems whose scratch does not
+ * fit are rejected with LIBPT_ERR_ARG before any work is queued (o = 8,
+ * v = 64 fits; the check is the exact footprint of the solve).
+ * The first call on a device loads the library's device code there (CUDA
+ * loads modules lazily), which reserves the array and the kernels' code, and
+ * looks up the array's device address: make that first call -- any size
+ * that fits -- before a pool allocator claims the device's memory and before
+ * any stream capture.  A call synchronizes the stream it is given (it reads
+ * back whether f_ov is zero and the energies), not the device.
  * Every call shares the array: calls whose work overlaps on the GPU race and
  * give wrong results -- serialize them. */
 #define LIBPT_STATIC_SCRATCH_BYTES (64ull << 20)

@@ -66,6 +66,25 @@ int libpt_server_submit(libpt_server *s, int kind, size_t oa, size_t va,
 int libpt_server_wait(libpt_server *s, uint64_t ticket, double timeout_s,
                       double *energy, double *latency_s);
 
+/* Cancels a solve.  A queued solve leaves the queue at once; one whose plan
+ * is being created, or whose triples are running, gets no further rounds
+ * and ends as soon as its rounds in flight retire, returning its block to
+ * the pool.  Either way libpt_server_wait then reports LIBPT_ERR_CANCELLED
+ * (no energy).  A solve that has already ended keeps its result; returns
+ * LIBPT_OK (LIBPT_ERR_ARG for an unknown ticket).  The other solves are not
+ * affected: their energies stay bitwise those they have alone. */
+int libpt_server_cancel(libpt_server *s, uint64_t ticket);
+
+/* Where an ended solve's latency went, in seconds, times[0..3]: waiting for
+ * admission (a block of its footprint in the pool and a resident slot),
+ * preparing (plan creation in its block: uploads, operand preparation,
+ * slice choice, tuning), waiting for its first round, and running (from its
+ * first round's launch to its energy, its rounds interleaved with the other
+ * resident solves').  They add up to the latency libpt_server_wait reports.
+ * LIBPT_ERR_TIMEOUT if the solve has not ended. */
+int libpt_server_solve_times(libpt_server *s, uint64_t ticket,
+                             double *times);
+
 /* Non-blocking: *released = 1 once the server no longer reads the solve's
  * arguments (its operands are resident in the pool, or it ended), so the
  * caller may free or reuse them before the solve completes. */

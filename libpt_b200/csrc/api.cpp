@@ -15,14 +15,16 @@ namespace {
 void *(*g_malloc)(size_t) = malloc;
 void (*g_free)(void *) = free;
 
-// Precision of the FP32 (*_mp) entry points: the FP64 engine (at least as
-// accurate as the reference's FP32 path), or the 3xTF32 tensor-core form
-// when LIBPT_MP_PRECISION=tf32x3 (5x faster; its tensor-core FP32
-// accumulation leaves ~1e-6 relative error in synthetic energies).
+// Precision of the FP32 (*_mp) entry points: the FP32 tensor-core form (5
+// INT8 digit planes, exact accumulation), or under LIBPT_MP_PRECISION the
+// FP64 engine (=fp64) or the 3xTF32 form (=tf32x3; its truncating FP32
+// accumulation leaves ~2e-6 relative error in synthetic energies).
 int mp_precision() {
   const char *e = getenv("LIBPT_MP_PRECISION");
   if (e && (e[0] == 't' || e[0] == 'T')) return LIBPT_PREC_TF32X3;
-  return LIBPT_PREC_FP64;
+  if (e && (e[0] == 'f' || e[0] == 'F') && e[1] == 'p' && e[2] == '6')
+    return LIBPT_PREC_FP64;
+  return LIBPT_PREC_FP32;
 }
 
 // Precision of the FP64 entry points: the FP64 engine, or emulated FP64
@@ -65,9 +67,11 @@ double host_solve(const char *name, int kind, size_t oa, size_t va, size_t ob,
   if (!r && ptb::profile_enabled())
     fprintf(stderr,
             "libpt: %s oa=%zu va=%zu ob=%zu vb=%zu: upload %.3f s, prepare "
-            "%.3f s, tune %.3f s, create %.3f s, triples %.3f s\n",
+            "%.3f s, tune %.3f s, create %.3f s, triples %.3f s, "
+            "precision %d, slices %d\n",
             name, oa, va, ob, vb, p->prof_upload, p->prof_prepare,
-            p->prof_tune, t1 - t0, ptb::wall_seconds() - t1);
+            p->prof_tune, t1 - t0, ptb::wall_seconds() - t1, p->precision,
+            p->precision == LIBPT_PREC_EMU64 ? p->slices : 0);
   ptb::plan_destroy(p);
   cudaStreamDestroy(st);
   if (r) fatal(name);
@@ -296,6 +300,7 @@ LIBPT_API int64_t libpt_plan_queue_length(const libpt_plan *plan) {
 }
 
 LIBPT_API int libpt_plan_slices(const libpt_plan *plan) {
+  // (the FP32 form runs as emulated FP64 with 4 slices)
   return plan && plan->precision == LIBPT_PREC_EMU64 ? plan->slices : 0;
 }
 

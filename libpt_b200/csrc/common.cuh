@@ -15,8 +15,13 @@ namespace ptb {
 enum : unsigned { ERR_WAIT_TIMEOUT = 1u };
 
 // Wall-clock limit of any single device-side wait.  One GEMM tile finishes in
-// well under a millisecond; two seconds only triggers on a logic error.
-constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;
+// well under a millisecond; two seconds only triggers on a logic error.  A
+// build may set another limit with -DLIBPT_WAIT_LIMIT_NS=...; mbar_wait also
+// takes a per-call limit (the wait probe of the self-test uses a short one).
+#ifndef LIBPT_WAIT_LIMIT_NS
+#define LIBPT_WAIT_LIMIT_NS 2000000000ull
+#endif
+constexpr unsigned long long WAIT_LIMIT_NS = LIBPT_WAIT_LIMIT_NS;
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
@@ -66,12 +71,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 // Wait until the phase with the given parity has completed.  Returns false
 // (and raises ERR_WAIT_TIMEOUT in *err) if that takes longer than
 // WAIT_LIMIT_NS; callers then stop issuing work and leave the kernel.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
-                                          unsigned *err) {
+__device__ __forceinline__ bool mbar_wait(
+    uint64_t *bar, uint32_t parity, unsigned *err,
+    unsigned long long limit_ns = WAIT_LIMIT_NS) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer_ns();
   while (!mbar_try_wait(bar, parity)) {
-    if (globaltimer_ns() - t0 > WAIT_LIMIT_NS) {
+    if (globaltimer_ns() - t0 > limit_ns) {
       atomicOr(err, ERR_WAIT_TIMEOUT);
       return false;
     }

@@ -12,14 +12,18 @@
 // the inputs (device pointers, pt.h layout) and receives the energy.
 //
 // The array is LIBPT_STATIC_SCRATCH_BYTES (64 MiB) of device memory that
-// every GPU on which this library's kernels are loaded keeps until the
-// process exits.  All calls share it: each call clears the parts that must
-// start at zero, later calls overwrite what earlier calls left, and two calls
-// whose work overlaps on the GPU (different streams or threads at once) race
-// on it and give wrong energies.
+// every GPU on which this file's device code is loaded keeps until the
+// process exits.  Under CUDA's lazy module loading that happens at the first
+// call on a device (the address lookup below loads it), so a caller whose
+// pool allocator claims the device's memory makes one call -- any size that
+// fits -- before creating its pool.  All calls share the array: each call
+// clears the parts that must start at zero, later calls overwrite what
+// earlier calls left, and two calls whose work overlaps on the GPU
+// (different streams or threads at once) race on it and give wrong
+// energies.  A call synchronizes the stream it is given (it reads whether
+// f_ov is zero and the energies back), not the device.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "plan.h"
@@ -32,36 +36,21 @@ static __device__ __align__(256) unsigned char
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void *g_scratch_addr[kMaxDevices] = {};
-
 // Device address of the scratch array on the current device.  In host code
 // the array's name is only a host-side stand-in, so the address is looked up
-// once per device (with that device current) and cached.
+// with the device current.  It is looked up on every call (cheap once this
+// file's device code is loaded) rather than cached: after a device reset the
+// code is loaded again, possibly at another address.  The first lookup on a
+// device loads this file's device code, which is when the array is reserved.
 int scratch_address(void **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) {
-    ptb::set_error(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+  if (e != cudaSuccess || !p) {
+    ptb::set_error(std::string("cudaGetSymbolAddress(static scratch): ") +
+                   cudaGetErrorString(e));
     return LIBPT_ERR_CUDA;
   }
-  if (dev < 0 || dev >= kMaxDevices) {
-    ptb::set_error("device index out of range");
-    return LIBPT_ERR_UNSUPPORTED;
-  }
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_static_scratch);
-    if (e != cudaSuccess || !p) {
-      ptb::set_error(std::string("cudaGetSymbolAddress(static scratch): ") +
-                     cudaGetErrorString(e));
-      return LIBPT_ERR_CUDA;
-    }
-    g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
+  *out = p;
   return LIBPT_OK;
 }
 
@@ -86,7 +75,9 @@ LIBPT_API int libpt_rpt_dev_static(size_t oa, size_t va, const double *d_ov,
       (oa > 4096 || va > 4096 || lower > (double)LIBPT_STATIC_SCRATCH_BYTES)
           ? (size_t)lower
           : ptb::plan_footprint(0, oa, va, oa, va, 0, LIBPT_PREC_FP64, false, 1);
-  if (oa > 4096 || va > 4096 || need > (size_t)LIBPT_STATIC_SCRATCH_BYTES) {
+  // (a footprint of 0 means the sizing pass rejected the arguments)
+  if (oa > 4096 || va > 4096 || need == 0 ||
+      need > (size_t)LIBPT_STATIC_SCRATCH_BYTES) {
     ptb::set_error("libpt_rpt_dev_static: o=" + std::to_string(oa) +
                    ", v=" + std::to_string(va) + " needs " +
                    std::to_string(need) + " bytes of scratch; the static "

@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "common.cuh"
 #include "plan.h"
 #include "pt.h"
 
@@ -369,4 +370,77 @@ LIBPT_API int libpt_selftest_variants(int precision) {
     }
     default: return 0;
   }
+}
+
+namespace {
+
+// Wait probe: a producer / consumer hand-off through a ring of four stages
+// (the pipelines of the contraction kernels in miniature), in which the
+// producer stops after `arrive` of the `stages` hand-offs -- a lost arrival,
+// as a TMA completion that never comes would be.  Every wait is bounded by
+// limit_ns: the consumer's wait for the missing hand-off runs out, raises
+// ERR_WAIT_TIMEOUT in *err and the kernel returns; nothing spins forever.
+__global__ void wait_probe_kernel(int stages, int arrive,
+                                  unsigned long long limit_ns, unsigned *err,
+                                  int *seen) {
+  __shared__ __align__(8) uint64_t full[4], empty[4];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 4; ++i) {
+      ptb::mbar_init(&full[i], 1);
+      ptb::mbar_init(&empty[i], 1);
+    }
+    ptb::mbar_fence_init();
+  }
+  __syncthreads();
+  if (lane != 0) return;
+  if (warp == 0) {          // producer
+    for (int s = 0; s < stages && s < arrive; ++s) {
+      const uint32_t ph = (s >> 2) & 1;
+      if (!ptb::mbar_wait(&empty[s & 3], ph ^ 1, err, limit_ns)) return;
+      ptb::mbar_arrive(&full[s & 3]);
+    }
+  } else if (warp == 1) {   // consumer
+    for (int s = 0; s < stages; ++s) {
+      const uint32_t ph = (s >> 2) & 1;
+      if (!ptb::mbar_wait(&full[s & 3], ph, err, limit_ns)) return;
+      atomicAdd(seen, 1);
+      ptb::mbar_arrive(&empty[s & 3]);
+    }
+  }
+}
+
+}  // namespace
+
+LIBPT_API int libpt_selftest_wait(int stages, int arrive, double limit_ms,
+                                  int *seen) {
+  if (stages < 1 || stages > 4096 || arrive < 0 || arrive > stages ||
+      !(limit_ms > 0.0) || limit_ms > 2000.0 || !seen) {
+    ptb::set_error("libpt_selftest_wait: bad arguments");
+    return LIBPT_ERR_ARG;
+  }
+  unsigned *buf = nullptr;   // [0]: error word, [1]: hand-offs seen
+  CK(cudaMalloc(&buf, 2 * sizeof(unsigned)));
+  cudaError_t ce = cudaMemset(buf, 0, 2 * sizeof(unsigned));
+  if (ce == cudaSuccess) {
+    wait_probe_kernel<<<1, 64>>>(stages, arrive,
+                                 (unsigned long long)(limit_ms * 1e6), buf,
+                                 reinterpret_cast<int *>(buf + 1));
+    ce = cudaGetLastError();
+  }
+  if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
+  unsigned h[2] = {0, 0};
+  if (ce == cudaSuccess) ce = cudaMemcpy(h, buf, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  if (ce != cudaSuccess) {
+    ptb::set_error(std::string("libpt_selftest_wait: ") + cudaGetErrorString(ce));
+    return LIBPT_ERR_CUDA;
+  }
+  *seen = (int)h[1];
+  if (h[0] & ptb::ERR_WAIT_TIMEOUT) {
+    ptb::set_error("libpt_selftest_wait: a device-side wait exceeded its "
+                   "time limit of " + std::to_string(limit_ms) + " ms");
+    return LIBPT_ERR_TIMEOUT;
+  }
+  return LIBPT_OK;
 }

@@ -106,7 +106,11 @@ struct Solve {
   int half = 0;                  // rounds can be in flight (next half)
   double remaining = 0.0;        // reference flops left to schedule
   bool done = false;
+  bool cancelled = false;        // libpt_server_cancel: stop and report so
   bool consumed = false;         // inputs copied (or the solve ended)
+  // phase marks (now_s): block granted, plan created (resident), first
+  // round launched
+  double t_admit = 0.0, t_ready = 0.0, t_first = 0.0;
   int status = LIBPT_OK;
   std::string error;             // message of a failure
   double energy = 0.0;
@@ -230,13 +234,19 @@ void admit_loop(libpt_server *S) {
       }
     }
     {
-      // wait for room: a free block and a resident slot
+      // wait for room: a free block and a resident slot (or a cancel)
       std::unique_lock<std::mutex> lk(S->mu);
       S->cv_admit.wait(lk, [&] {
-        return (int)S->resident.size() < S->max_active &&
-               S->pool.alloc(s->bytes, &s->off);
+        return s->cancelled || ((int)S->resident.size() < S->max_active &&
+                                S->pool.alloc(s->bytes, &s->off));
       });
       S->pending.pop_front();
+      if (s->cancelled) {
+        set_error("libpt_server: solve cancelled");
+        finish(S, s, LIBPT_ERR_CANCELLED);
+        continue;
+      }
+      s->t_admit = now_s();
       ++S->admitting;
       S->in_use += up256(s->bytes);
       S->peak = std::max(S->peak, S->in_use);
@@ -259,7 +269,18 @@ void admit_loop(libpt_server *S) {
     s->consumed = true;   // plan_create synchronized its uploads
     s->total = p->queue.size();
     s->remaining = plan_flops(p, 0, (int64_t)s->total);
+    s->t_ready = now_s();
     --S->admitting;
+    if (s->cancelled) {   // cancelled while its plan was being created
+      plan_destroy(p);
+      s->plan = nullptr;
+      S->pool.release(s->off, s->bytes);
+      S->in_use -= up256(s->bytes);
+      set_error("libpt_server: solve cancelled");
+      finish(S, s, LIBPT_ERR_CANCELLED);
+      S->cv_admit.notify_all();
+      continue;
+    }
     if (s->total == 0) {   // empty spaces: zero energy, nothing to run
       plan_destroy(p);
       s->plan = nullptr;
@@ -282,8 +303,17 @@ void admit_loop(libpt_server *S) {
 void complete(libpt_server *S, const std::shared_ptr<Solve> &s, bool err) {
   double e = 0.0;
   int r = err ? LIBPT_ERR_TIMEOUT : LIBPT_OK;
+  bool cancelled;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    cancelled = s->cancelled;
+  }
   if (err) set_error("libpt_server: a device-side wait of the solve's round "
                      "exceeded its time limit, or the round failed to launch");
+  if (!r && cancelled) {
+    set_error("libpt_server: solve cancelled");
+    r = LIBPT_ERR_CANCELLED;
+  }
   if (!r) r = plan_energy(s->plan, nullptr, 0, &e, S->read_st);
   plan_destroy(s->plan);
   std::lock_guard<std::mutex> lk(S->mu);
@@ -315,7 +345,8 @@ void retire(libpt_server *S, bool block) {
     {
       std::lock_guard<std::mutex> lk(S->mu);
       for (auto &s : rr.solves)
-        if (--s->inflight == 0 && s->next == s->total) fin.push_back(s);
+        if (--s->inflight == 0 && (s->next == s->total || s->cancelled))
+          fin.push_back(s);
     }
     cudaEventDestroy(rr.ev);
     S->inflight.pop_front();
@@ -329,11 +360,21 @@ void run_loop(libpt_server *S) {
     retire(S, false);
     // candidates: resident solves with triples to schedule and no round in
     // flight, least remaining work first
-    std::vector<std::shared_ptr<Solve>> cand;
+    std::vector<std::shared_ptr<Solve>> cand, drop;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      for (auto &s : S->resident)
+      for (auto &s : S->resident) {
+        if (s->cancelled) {   // no more rounds; ends once none is in flight
+          if (s->inflight == 0) drop.push_back(s);
+          continue;
+        }
         if (s->next < s->total && s->inflight < s->halves) cand.push_back(s);
+      }
+      if (!drop.empty()) {
+        lk.unlock();
+        for (auto &s : drop) complete(S, s, false);
+        continue;
+      }
       if (cand.empty() && S->inflight.empty()) {
         if (S->stop && S->pending.empty() && S->admitting == 0 &&
             S->resident.empty())
@@ -391,6 +432,7 @@ void run_loop(libpt_server *S) {
         continue;
       s->remaining -= plan_flops(p, (int64_t)s->next, (int64_t)taken);
       s->next += taken;
+      if (s->t_first == 0.0) s->t_first = now_s();
       s->half ^= 1;
       rr.solves.push_back(s);
     }
@@ -587,6 +629,56 @@ LIBPT_API int libpt_server_wait(libpt_server *S, uint64_t ticket,
   if (latency_s) *latency_s = s->t_done - s->t_submit;
   if (s->status != LIBPT_OK) set_error(s->error);
   return s->status;
+}
+
+LIBPT_API int libpt_server_cancel(libpt_server *S, uint64_t ticket) {
+  if (!S) return LIBPT_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->by_id.find(ticket);
+  if (it == S->by_id.end()) {
+    set_error("libpt_server_cancel: unknown ticket");
+    return LIBPT_ERR_ARG;
+  }
+  std::shared_ptr<Solve> s = it->second;
+  if (s->done || s->cancelled) return LIBPT_OK;
+  s->cancelled = true;
+  // queued behind the solve the admitter holds: leave the queue now (the
+  // admitter itself ends the one at the front of the queue)
+  auto q = std::find(S->pending.begin(), S->pending.end(), s);
+  if (q != S->pending.end() && q != S->pending.begin()) {
+    S->pending.erase(q);
+    set_error("libpt_server: solve cancelled");
+    finish(S, s, LIBPT_ERR_CANCELLED);
+  }
+  S->cv_admit.notify_all();
+  S->cv_run.notify_all();
+  return LIBPT_OK;
+}
+
+LIBPT_API int libpt_server_solve_times(libpt_server *S, uint64_t ticket,
+                                       double *times) {
+  if (!S || !times) return LIBPT_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->by_id.find(ticket);
+  if (it == S->by_id.end()) {
+    set_error("libpt_server_solve_times: unknown ticket");
+    return LIBPT_ERR_ARG;
+  }
+  const Solve &s = *it->second;
+  if (!s.done) {
+    set_error("libpt_server_solve_times: the solve has not ended");
+    return LIBPT_ERR_TIMEOUT;
+  }
+  // phases that did not happen (a solve refused or cancelled early) take
+  // the time of the next one that did
+  const double admit = s.t_admit ? s.t_admit : s.t_done;
+  const double ready = s.t_ready ? s.t_ready : s.t_done;
+  const double first = s.t_first ? s.t_first : s.t_done;
+  times[0] = admit - s.t_submit;
+  times[1] = ready - admit;
+  times[2] = first - ready;
+  times[3] = s.t_done - first;
+  return LIBPT_OK;
 }
 
 LIBPT_API int libpt_server_inputs_released(libpt_server *S, uint64_t ticket,

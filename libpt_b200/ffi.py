@@ -20,11 +20,14 @@ KIND_ID = {k: i for i, k in enumerate(KINDS)}
 LIBPT_OK = 0
 LIBPT_ERR_NOMEM = 2
 LIBPT_ERR_TIMEOUT = 4
+LIBPT_ERR_CANCELLED = 6
 ERRORS = {1: "LIBPT_ERR_ARG", 2: "LIBPT_ERR_NOMEM", 3: "LIBPT_ERR_CUDA",
-          4: "LIBPT_ERR_TIMEOUT", 5: "LIBPT_ERR_UNSUPPORTED"}
+          4: "LIBPT_ERR_TIMEOUT", 5: "LIBPT_ERR_UNSUPPORTED",
+          6: "LIBPT_ERR_CANCELLED"}
 PREC_FP64 = 0
 PREC_TF32X3 = 1
 PREC_EMU64 = 2          # | (slices << 8), slices 4..7; 0: chosen for 1 uEh
+PREC_FP32 = 3           # FP32 tensor-core form (5 INT8 digit planes)
 
 _lib = None
 
@@ -95,6 +98,10 @@ def lib():
     L.libpt_selftest_variants.argtypes = [ctypes.c_int]
     L.libpt_kernel_bench.restype = ctypes.c_int
     L.libpt_kernel_bench.argtypes = [ctypes.c_int] * 5 + [dp, dp]
+    L.libpt_selftest_wait.restype = ctypes.c_int
+    L.libpt_selftest_wait.argtypes = [ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double,
+                                      ctypes.POINTER(ctypes.c_int)]
     # serving (pt_serve.h)
     L.libpt_footprint.restype = sz
     L.libpt_footprint.argtypes = [ctypes.c_int] + [sz] * 4 + [ctypes.c_int] * 3 + [sz]
@@ -106,6 +113,11 @@ def lib():
                                       [ctypes.POINTER(ctypes.c_uint64)])
     L.libpt_server_wait.restype = ctypes.c_int
     L.libpt_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, dp, dp]
+    L.libpt_server_cancel.restype = ctypes.c_int
+    L.libpt_server_cancel.argtypes = [vp, ctypes.c_uint64]
+    L.libpt_server_solve_times.restype = ctypes.c_int
+    L.libpt_server_solve_times.argtypes = [vp, ctypes.c_uint64,
+                                           ctypes.POINTER(ctypes.c_double)]
     L.libpt_server_inputs_released.restype = ctypes.c_int
     L.libpt_server_inputs_released.argtypes = [vp, ctypes.c_uint64,
                                                ctypes.POINTER(ctypes.c_int)]
@@ -193,6 +205,35 @@ def selftest_variants(precision):
     return lib().libpt_selftest_variants(precision)
 
 
+def selftest_wait(stages, arrive, limit_ms):
+    """(status code, hand-offs seen) of the bounded-wait probe
+    (libpt_selftest_wait): the producer stops after `arrive` of `stages`
+    hand-offs; a missing one makes the wait run out (LIBPT_ERR_TIMEOUT)."""
+    seen = ctypes.c_int(-1)
+    code = lib().libpt_selftest_wait(stages, arrive, limit_ms,
+                                     ctypes.byref(seen))
+    return code, seen.value
+
+
+HOST_MALLOC = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_size_t)
+HOST_FREE = ctypes.CFUNCTYPE(None, ctypes.c_void_p)
+
+
+def set_host_allocator(malloc_fn=None, free_fn=None):
+    """Installs host allocation hooks (libpt_set_malloc / libpt_set_free,
+    src/misc.c:33-47): Python callables, wrapped as C function pointers and
+    kept alive here; None restores malloc / free."""
+    global _hooks
+    m = HOST_MALLOC(malloc_fn) if malloc_fn else None
+    f = HOST_FREE(free_fn) if free_fn else None
+    _hooks = (m, f)
+    lib().libpt_set_malloc(ctypes.cast(m, ctypes.c_void_p) if m else None)
+    lib().libpt_set_free(ctypes.cast(f, ctypes.c_void_p) if f else None)
+
+
+_hooks = (None, None)
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
                 ("failed", ctypes.c_uint64), ("rounds", ctypes.c_uint64),
@@ -258,6 +299,18 @@ class Server:
             self._keep.pop(ticket, None)
         check(code)
         return e.value, lat.value
+
+    def cancel(self, ticket):
+        """Cancels a solve (libpt_server_cancel); its wait then raises
+        LIBPT_ERR_CANCELLED unless it had already ended."""
+        check(lib().libpt_server_cancel(self.h, ticket))
+
+    def times(self, ticket):
+        """(admission wait, preparation, wait for the first round, running)
+        seconds of an ended solve (libpt_server_solve_times)."""
+        t = (ctypes.c_double * 4)()
+        check(lib().libpt_server_solve_times(self.h, ticket, t))
+        return tuple(t)
 
     def release_inputs(self):
         """Drops the references to inputs the server no longer reads;

@@ -46,10 +46,12 @@ def _load(path, prefix):
 
 
 def build(ref=True):
-    """Compile the checkers (the reference only when its tree is present)."""
+    """Compile the checkers; the reference build too when the environment
+    names the reference's source directory (REFSRC) and it exists."""
     targets = ["oracle"]
-    if ref and os.path.isdir(os.environ.get("REFSRC", "/root/reference/src")):
-        targets.append("ref")
+    refsrc = os.environ.get("REFSRC", "")
+    if ref and refsrc and os.path.isdir(refsrc):
+        targets += ["ref", "REFSRC=" + refsrc]
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 

@@ -158,7 +158,11 @@ def convert(name, path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    # the reference checkout (whose tests/ holds the .dat fixtures): the
+    # first argument, else the REFROOT environment variable
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFROOT", "")
+    if not ref or not os.path.isdir(os.path.join(ref, "tests")):
+        sys.exit("usage: make_golden.py <reference checkout> (or REFROOT=...)")
     from tests.golden.fixtures import reference_energy
     energies = {}
     for name in NAMES:

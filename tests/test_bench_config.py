@@ -40,12 +40,27 @@ def test_sharded_sample_is_denser_with_ranks():
     assert eight["parallelism"].startswith("triples sharded x8")
 
 
-def test_cpu_extrapolation_is_the_workload_flops_over_the_rate():
+def test_cpu_extrapolation_scales_each_kind_by_its_rate():
+    """Same-spin triples at the same-spin rate, mixed-spin triples at the
+    mixed-spin rate: with equal rates the extrapolation is the workload's
+    flops over that rate; the triple counts are C(o,3) and C(o,2) o."""
     a = args_of()
-    x = bench.extrapolation(a, 0.08)
+    v = 477
+    r = dict(flops_aaa=bench.aaa_flops(3, v), seconds_aaa=bench.aaa_flops(3, v) / 0.08e12,
+             flops_aab=bench.aab_flops(2, v, 1, v),
+             seconds_aab=bench.aab_flops(2, v, 1, v) / 0.08e12)
+    x = bench.extrapolation(a, r)
     assert abs(x["extrapolated_solve_seconds"] -
-               bench.rpt_flops(45, 477) / 0.08e12) < 1e-6
+               bench.rpt_flops(45, 477) / 0.08e12) < 1e-6 * x["extrapolated_solve_seconds"]
     assert x["extrapolation"].startswith("extrapolated: rpt o=45 v=477")
+    # a mixed-spin rate twice as high halves the mixed-spin part
+    r2 = dict(r, seconds_aab=r["seconds_aab"] / 2)
+    t_aaa = 14190 * bench.aaa_flops(45, v) / 0.08e12
+    t_aab = 44550 * bench.aab_flops(45, v, 45, v) / 0.08e12
+    assert abs(bench.extrapolation(a, r2)["extrapolated_solve_seconds"] -
+               (t_aaa + t_aab / 2)) < 1e-6 * t_aaa
+    assert abs(14190 * bench.aaa_flops(45, v) + 44550 * bench.aab_flops(45, v, 45, v)
+               - bench.rpt_flops(45, v)) < 1e-9 * bench.rpt_flops(45, v)
 
 
 def test_reference_single_thread_run_matches_the_threaded_one():
@@ -66,7 +81,25 @@ def test_reference_single_thread_run_matches_the_threaded_one():
 
 def test_precision_forms_cover_every_form():
     from libpt_b200 import ffi
-    names = [f[0] for f in bench.precision_forms(ffi)]
+    forms = bench.precision_forms(ffi, (4, 5, 6, 7))
+    names = [f[0] for f in forms]
     assert names == ["fp64", "emu64_s4", "emu64_s5", "emu64_s6", "emu64_s7",
-                     "emu64_auto", "tf32x3"]
-    assert [f[2] for f in bench.precision_forms(ffi)].count(True) == 1
+                     "emu64_auto", "fp32_tc", "fp64_on_fp32_inputs", "tf32x3"]
+    # the FP32-input forms: the FP32 tensor-core form, its floor, 3xTF32
+    assert [f[0] for f in forms if f[2]] == ["fp32_tc", "fp64_on_fp32_inputs",
+                                             "tf32x3"]
+    assert dict((f[0], f[1]) for f in forms)["fp32_tc"] == ffi.PREC_FP32
+
+
+def test_precision_cases_have_reference_energies():
+    """Every case of the precision table has committed reference energies
+    (FP64 and the reference's FP32 *_mp) for the seed the bench uses."""
+    refs = bench.reference_energies()
+    for name, kind, sz, seed in bench.PRECISION_CASES:
+        if name not in refs:
+            import pytest
+            pytest.skip(f"{name}: reference energies not generated yet")
+        r = refs[name]
+        assert r["kind"] == kind and tuple(r["sizes"]) == sz
+        assert r["seed"] == seed
+        assert r["fp64"]["energy"] != 0.0 and r["fp32_mp"]["energy"] != 0.0

@@ -58,11 +58,53 @@ def test_static_matches_allocating_entry_twice():
     assert free_after == free_before
 
 
-def test_static_rejects_systems_beyond_its_scratch():
+@pytest.mark.parametrize("o,v", [(30, 300), (8, 78)])
+def test_static_rejects_systems_beyond_its_scratch(o, v):
+    """o=30, v=300 fails the cheap lower bound; o=8, v=78 passes it (35 MiB)
+    but its exact footprint (67 MiB, sizing pass) exceeds the 64 MiB."""
     f = _bind()
     e = ctypes.c_double(0.0)
     # sizes are checked before any pointer is used; NULL pointers keep the
     # call harmless even if the check were missing
-    rc = f(30, 300, *([None] * 7), None, ctypes.byref(e))
+    rc = f(o, v, *([None] * 7), None, ctypes.byref(e))
     assert rc == 1
     assert b"scratch" in ffi.lib().libpt_last_error()
+
+
+FRESH = r"""
+import ctypes, sys
+sys.path.insert(0, %r)
+import numpy as np, torch
+from libpt_b200 import ffi, synth
+from tests.test_zz_no_alloc import _bind, _static_solve
+torch.cuda.init()
+case = synth.rpt_case(4, 20, seed=3)
+t = {n: torch.as_tensor(np.ascontiguousarray(case[n])).to(
+    device="cuda", dtype=torch.float64) for n in ffi.PT_ARGS}
+torch.cuda.synchronize()
+f = _bind()
+free = [torch.cuda.mem_get_info()[0]]
+for _ in range(2):
+    rc, e = _static_solve(f, case, t)
+    assert rc == 0, ffi.lib().libpt_last_error()
+    torch.cuda.synchronize()
+    free.append(torch.cuda.mem_get_info()[0])
+print(free[0] - free[1], free[1] - free[2])
+"""
+
+
+def test_first_call_reserves_the_scratch_once():
+    """In a fresh process: the first call on the device (which loads the
+    library's device code) takes the static array's memory, at least
+    LIBPT_STATIC_SCRATCH_BYTES; the second call takes none.  A caller whose
+    pool allocator claims the device's memory makes its first call before
+    creating the pool."""
+    import os
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, "-c", FRESH % os.getcwd()],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    first, second = map(int, r.stdout.split()[-2:])
+    assert first >= 64 << 20, first
+    assert second == 0
