@@ -63,6 +63,7 @@ O_FULL, V_FULL = 45, 477      # the workload (restricted, all-electron)
 STRIDE = 211                  # triples-queue sampling stride of one step
 O_E2E = 4                     # full solves through the host API
 O_CPU = 0                     # the reference's host sample (0: per kind)
+CPU_FULL_O = 4                # full solve in the reference's own layout
 
 
 def parse():
@@ -96,6 +97,10 @@ def parse():
     ap.add_argument("--serve-rates", default="20,50,100",
                     help="Poisson arrival rates of the served stream (req/s)")
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run the served stream alone (e.g. the 300-request "
+                         "version: --serve-only --serve-requests 300, "
+                         "~15 min) and print its JSON line")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the precision table (unrestricted (T) and (fT))")
     ap.add_argument("--no-rft", action="store_true",
@@ -281,7 +286,8 @@ def cpu_worker(args):
         for _ in range(args.cpu_reps):
             e = oracle.solve(ref, case)
         dt = (time.perf_counter() - t0) / args.cpu_reps
-        print(json.dumps(dict(seconds=dt, flops=rpt_flops(args.cpu_o, args.v),
+        print(json.dumps(dict(o=args.cpu_o, v=args.v, seconds=dt,
+                              flops=rpt_flops(args.cpu_o, args.v),
                               energy=e)))
         return
     v = args.v
@@ -340,6 +346,13 @@ def extrapolation(args, r):
     o, v = args.o, args.v
     n_aaa = o * (o - 1) * (o - 2) // 6
     n_aab = o * (o - 1) // 2 * o
+    if "seconds_aaa" not in r:   # a full solve of both kinds: its rate
+        rate = r["flops"] / r["seconds"]
+        return dict(
+            extrapolated_solve_seconds=rpt_flops(o, v) / rate,
+            extrapolation=f"extrapolated: rpt o={o} v={v} reference flops "
+                          f"({rpt_flops(o, v):.4g}) over the rate of the "
+                          f"o={r['o']} v={v} solve (both kinds of triple)")
     rate_aaa = r["flops_aaa"] / r["seconds_aaa"]
     rate_aab = r["flops_aab"] / r["seconds_aab"]
     secs = (n_aaa * aaa_flops(o, v) / rate_aaa
@@ -406,10 +419,15 @@ def run_reference(args, d):
             "oracle/_ref/libpt_ref.so was not built (needs the reference "
             "source tree at build time)"))))
         return
+    # once, before the steps: a full o=4 solve in the reference's own
+    # full-solve layout (OpenMP over triples, one BLAS thread each), whose
+    # rate the per-step sample's threaded-BLAS layout does not reach
+    full = run_cpu(CPU_FULL_O, args.v, 1, "omp")
     t0 = time.perf_counter()
     res = run_cpu(0, args.v, max(args.steps, 1), warmup=args.warmup)
     wall = time.perf_counter() - t0
     val = res["flops"] / res["seconds"] / 1e12
+    full_rate = full["flops"] / full["seconds"] / 1e12
     line = dict(
         metric="(T) TFLOP/s, restricted o=45 v=477 workload (reference "
                "dgemm flops per second)",
@@ -429,6 +447,13 @@ def run_reference(args, d):
                           **extrapolation(args, res)),
         e2e=dict(value=val, unit="TFLOP/s", h2d_bytes_per_step=0,
                  d2h_bytes_per_step=0),
+        reference_full_solve_layout=dict(
+            tflops=full_rate, seconds=full["seconds"], cores=full["cores"],
+            sample=f"full libpt_rpt solve o={CPU_FULL_O} v={args.v}, OpenMP "
+                   f"over triples on {full['cores']} threads, OpenBLAS 1 "
+                   "thread (run once before the steps)",
+            ratio_to_step_rate=full_rate / val,
+            **extrapolation(args, full)),
         wall_seconds=wall)
     print(json.dumps(line))
 
@@ -442,6 +467,12 @@ def run_ours(args, d):
     dev = torch.device("cuda", d.local)
     props = torch.cuda.get_device_properties(dev)
     gpu_id = "GPU-" + str(props.uuid) if getattr(props, "uuid", None) else "0"
+    if args.serve_only:   # the served stream alone (one JSON line)
+        if d.rank == 0:
+            print(json.dumps(dict(metric="served stream", serving=run_serving(
+                args, torch, gpu_id))))
+        d.close()
+        return
 
     peak64 = fp64_peak_tflops(torch)
 
@@ -569,11 +600,17 @@ def run_ours(args, d):
     cpu = None
     if not args.no_cpu and d.world == 1 and d.rank == 0:
         try:
-            r = run_cpu(0, args.v, 1)
+            # the reference's own full-solve layout (OpenMP over triples,
+            # one BLAS thread per triple; src/pt.c:227-230) on a full solve
+            # with both kinds of triple: 4 same-spin + 24 mixed-spin
+            r = run_cpu(CPU_FULL_O, args.v, 1, "omp")
             rate = r["flops"] / r["seconds"] / 1e12
             cpu = dict(value=rate, unit="TFLOP/s",
                        cores=r["cores"], kind="reference",
-                       sample=sample_description(r),
+                       sample=f"reference libpt_rpt (oracle/_ref) full solve "
+                              f"o={CPU_FULL_O} v={args.v} ({r['seconds']:.1f}"
+                              f" s), OpenMP over triples on {r['cores']} "
+                              "threads, OpenBLAS 1 thread",
                        **extrapolation(args, r))
         except Exception as ex:   # report, do not fail the bench
             cpu = dict(value=None, unit="TFLOP/s", cores=os.cpu_count(),

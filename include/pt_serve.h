@@ -16,8 +16,9 @@
  *    rounds -- one GEMM launch per kernel variant over the triples of many
  *    solves, one energy-epilogue launch, one reduction -- with the
  *    solves of least remaining work first; a request that arrives while
- *    others run joins the next round.  Rounds of small solves replay
- *    CUDA graphs captured once per variant set.
+ *    others run joins the next round.  Rounds replay CUDA graphs captured
+ *    once per set of kernel variants (the first round of a set launches
+ *    directly and captures).
  *  - Each solve's energy is the same as libpt_plan / libpt_{r,u}{pt,ft}
  *    compute for it alone (per-triple energies in fixed order, summed in
  *    queue order): bitwise, whatever else shares its rounds.

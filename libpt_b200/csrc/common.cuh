@@ -247,4 +247,78 @@ __device__ __forceinline__ int find_entry(const T *v, int n, int x,
   return lo;
 }
 
+// ---- device-resident tile queue ---------------------------------------------
+//
+// The reference hands triples to OpenMP threads one at a time
+// (schedule(dynamic), src/pt.c:228, 353).  Here the CTAs of a persistent
+// GEMM launch take output tiles one at a time from the counter in the
+// launch's work list (GemmList::next): a CTA's producer thread takes its
+// next tile while the current one is still being staged, and hands the
+// index to the CTA's other roles through a small ring in shared memory
+// (slot `full` barrier: the index is written; `empty` barrier: every
+// consumer has read it).  -1 ends the sequence.  Tiles of uneven cost (jobs
+// of different K, rounds mixing solves) then spread over the SMs instead of
+// being dealt round-robin in advance.  Every wait is bounded.
+constexpr int TQ_SLOTS = 4;
+
+struct TileRing {
+  uint64_t full[TQ_SLOTS], empty[TQ_SLOTS];
+  int tile[TQ_SLOTS];
+};
+
+// Thread 0, before the CTA's first barrier: `consumers` arrivals free a slot.
+__device__ __forceinline__ void tq_init(TileRing *r, uint32_t consumers) {
+  for (int s = 0; s < TQ_SLOTS; ++s) {
+    mbar_init(&r->full[s], 1);
+    mbar_init(&r->empty[s], consumers);
+  }
+}
+
+// The next tile of the launch (may be >= ntiles: none left).
+__device__ __forceinline__ int tq_take(GemmList *l) {
+  return atomicAdd(&l->next, 1);
+}
+
+// Producer: publishes tile t (or -1) in the next slot.
+__device__ __forceinline__ bool tq_put(TileRing *r, int &slot, uint32_t &ph,
+                                       int t, unsigned *err) {
+  if (!mbar_wait(&r->empty[slot], ph ^ 1u, err)) return false;
+  r->tile[slot] = t;
+  mbar_arrive(&r->full[slot]);   // release: the index is visible after it
+  if (++slot == TQ_SLOTS) {
+    slot = 0;
+    ph ^= 1u;
+  }
+  return true;
+}
+
+// Consumer (every thread of a consuming warp calls it; lane 0 frees the
+// slot for the warp): the next tile index, -1 at the end or on a timeout.
+__device__ __forceinline__ int tq_get(TileRing *r, int &slot, uint32_t &ph,
+                                      unsigned *err, bool warp_arrives) {
+  if (!mbar_wait(&r->full[slot], ph, err)) return -1;
+  const int t = r->tile[slot];
+  if (warp_arrives) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) mbar_arrive(&r->empty[slot]);
+  } else {
+    mbar_arrive(&r->empty[slot]);
+  }
+  if (++slot == TQ_SLOTS) {
+    slot = 0;
+    ph ^= 1u;
+  }
+  return t;
+}
+
+// Producer, after its last take: the last CTA of the launch to get here
+// resets the list's counters, so the next launch of the same list (a
+// replayed graph, repeated self-test launches) starts from tile 0.
+__device__ __forceinline__ void tq_finish(GemmList *l) {
+  if (atomicAdd(&l->done, 1) == (int)gridDim.x - 1) {
+    atomicExch(&l->next, 0);
+    atomicExch(&l->done, 0);
+  }
+}
+
 }  // namespace ptb

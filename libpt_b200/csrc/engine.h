@@ -70,9 +70,15 @@ struct LaunchMaps {
 // changes.  Jobs are sorted by tile_begin; ntiles = total tiles.  Kernels
 // also take the jobs array itself as a (restrict) parameter, equal to
 // list->jobs, so the compiler may keep job fields across their stores.
+// The list is also the launch's tile queue: the CTAs of the DMMA and the
+// one-CTA INT8 kernels take tiles by incrementing `next` (the reference's
+// schedule(dynamic) over triples, src/pt.c:228, 353, on the device), and the
+// last CTA to finish resets `next` and `done` to zero for the next launch of
+// the same list; the host writes both as zero.
 struct GemmList {
   const GemmJob *jobs;
   int32_t njobs, ntiles;
+  int32_t next, done;
 };
 
 // Persistent grid of the GEMM kernels (one CTA per SM).
@@ -85,7 +91,7 @@ size_t gemm_smem_bytes(int bm);
 //               ntiles) as kernel parameters (direct launches);
 //   pm == null: maps in device memory (GemmJob::maps) and the counts read
 //               from d_list (fixed parameters: CUDA graph replay).
-cudaError_t gemm_dmma_launch(const GemmJob *d_jobs, const GemmList *d_list,
+cudaError_t gemm_dmma_launch(const GemmJob *d_jobs, GemmList *d_list,
                              int njobs, int ntiles, const LaunchMaps *pm,
                              int bm, int grid, unsigned *d_err,
                              cudaStream_t st);
@@ -120,7 +126,7 @@ struct TcProducts {           // acc[c] += A_plane[pa] * B_plane[pb]^T
 
 int tc_kchunk_elems(int kind);   // K elements per pipeline stage (TF32)
 // 3xTF32: planes {hi, lo} in separate maps (2i, 2i+1), products from prods.
-cudaError_t gemm_tc_launch(const GemmJob *d_jobs, const GemmList *d_list,
+cudaError_t gemm_tc_launch(const GemmJob *d_jobs, GemmList *d_list,
                            int njobs, int ntiles, const LaunchMaps *pm,
                            int grid, const TcProducts &prods, unsigned *d_err,
                            cudaStream_t st);
@@ -153,7 +159,7 @@ inline int64_t i8_kpad(int64_t K) {
 // their number (0 for an unsupported count).
 int i8_tiles(int slices, const I8Tile **out);
 cudaError_t gemm_i8_launch(int slices, I8Tile tile, const GemmJob *d_jobs,
-                           const GemmList *d_list, int njobs, int ntiles,
+                           GemmList *d_list, int njobs, int ntiles,
                            const LaunchMaps *pm, int grid, unsigned *d_err,
                            cudaStream_t st);
 

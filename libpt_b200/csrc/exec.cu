@@ -59,8 +59,8 @@ void ExecTiming::clear() {
 namespace {
 
 // Fixed header slots at the start of the descriptor buffer.
-constexpr size_t SLOT = 16;
-constexpr size_t HDR = 256;
+constexpr size_t SLOT = 32;
+constexpr size_t HDR = 512;
 static_assert(sizeof(GemmList) <= SLOT && sizeof(EpiList) <= SLOT &&
                   sizeof(RedList) <= SLOT,
               "list headers fit their slots");
@@ -136,7 +136,7 @@ int Executor::launch_all(const std::vector<GemmGroup> &groups,
   if (timing) CK(cudaEventRecord(ev[0], st_));
   int g = 0;
   for (const GemmGroup &grp : groups) {
-    const GemmList *lst = reinterpret_cast<const GemmList *>(d_buf_ + gemm_slot(g));
+    GemmList *lst = reinterpret_cast<GemmList *>(d_buf_ + gemm_slot(g));
     int grid = GEMM_GRID;
     if (!fixed) {
       int tiles = 0;
@@ -289,7 +289,7 @@ int Executor::run(Round &r, unsigned *d_err, ExecTiming *timing,
   for (size_t g = 0; g < groups.size(); ++g) {
     const std::vector<GemmJob> &jobs = r.gemm[groups[g]];
     std::memcpy(h + goff[g], jobs.data(), jobs.size() * sizeof(GemmJob));
-    GemmList l;
+    GemmList l{};
     l.jobs = reinterpret_cast<const GemmJob *>(d_buf_ + goff[g]);
     l.njobs = (int32_t)jobs.size();
     l.ntiles = jobs.empty() ? 0

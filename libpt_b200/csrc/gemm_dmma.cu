@@ -18,15 +18,18 @@
 // so the fragment loads of a half-warp read 16 consecutive doubles (no bank
 // conflicts) for both operands.
 //
-// Persistent: GEMM_GRID CTAs stride over the launch's tiles, read with the
-// jobs from a device-memory work list (GemmList), so one launch can hold the
-// triples of many plans and a captured CUDA graph can be replayed with new
-// lists.  The producer runs ahead into the next tile's operands while the
-// consumers store the current one.  Each job carries its plan's tensor maps
-// (device memory; fenced before first use).
+// Persistent: GEMM_GRID CTAs take the launch's tiles one at a time from the
+// tile queue of a device-memory work list (GemmList; common.cuh tq_*), so
+// one launch can hold the triples of many plans, tiles of uneven length
+// spread over the SMs, and a captured CUDA graph can be replayed with new
+// lists.  The producer takes a tile, hands its index to the consumer warps
+// through a shared-memory ring, and runs ahead into the next tile's operands
+// while the consumers store the current one.  Each job carries its plan's
+// tensor maps (device memory; fenced before first use).
 //
-// Tiles are numbered M-tile fastest inside a job, so the CTAs that share one
-// B (OVVV) tile run at the same time and the tile is fetched from DRAM once.
+// Tiles are numbered M-tile fastest inside a job and taken in order, so the
+// CTAs that share one B (OVVV) tile run at the same time and the tile is
+// fetched from DRAM once.
 #include "common.cuh"
 #include "engine.h"
 
@@ -50,21 +53,21 @@ template <int BM, bool PM>
 __device__ __forceinline__ void dmma_body(const LaunchMaps *pm,
                                           const GemmJob *__restrict__ jobs,
                                           const int njobs, const int ntiles,
-                                          unsigned *err) {
+                                          GemmList *list, unsigned *err) {
   constexpr int MF = BM / 32;   // m16 fragments per warp (2 warp rows)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   double *sA = reinterpret_cast<double *>(smem_raw);
   double *sB = sA + ST * BM * BK;
   uint64_t *full = reinterpret_cast<uint64_t *>(sB + ST * BK * BN);
   uint64_t *empty = full + ST;
-
-
+  TileRing *tq = reinterpret_cast<TileRing *>(empty + ST);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < ST; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], NCW);
     }
+    tq_init(tq, NCW);
     mbar_fence_init();
   }
   __syncthreads();
@@ -76,8 +79,17 @@ __device__ __forceinline__ void dmma_body(const LaunchMaps *pm,
       uint32_t phase = 0;
       int issued = 0;
       bool ok = true;
+      int qslot = 0;
+      uint32_t qph = 0;
       MapSource<PM> ms(pm);
-      for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+      // tiles from the launch's queue; the next one is taken while the
+      // current one is staged
+      int tile = tq_take(list);
+      while (ok) {
+        if (!tq_put(tq, qslot, qph, tile < ntiles ? tile : -1, err) ||
+            tile >= ntiles)
+          break;
+        const int next_tile = tq_take(list);
         const GemmJob &job =
             jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
         const int local = tile - job.tile_begin;
@@ -112,7 +124,9 @@ __device__ __forceinline__ void dmma_body(const LaunchMaps *pm,
             }
           }
         }
+        tile = next_tile;
       }
+      tq_finish(list);
       // Drain: do not leave the CTA while copies issued by it are in flight.
       const int tail = issued < ST ? issued : ST;
       for (int d = 0; d < tail; ++d) {
@@ -142,7 +156,11 @@ __device__ __forceinline__ void dmma_body(const LaunchMaps *pm,
   int stage = 0;
   uint32_t phase = 0;
   bool ok = true;
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+  int qslot = 0;
+  uint32_t qph = 0;
+  for (;;) {
+    const int tile = tq_get(tq, qslot, qph, err, true);
+    if (tile < 0) break;
     const GemmJob &job =
         jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
     const int local = tile - job.tile_begin;
@@ -222,19 +240,19 @@ template <int BM>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     gemm_dmma_kernel(const __grid_constant__ LaunchMaps pm,
                      const GemmJob *__restrict__ jobs, int njobs, int ntiles,
-                     unsigned *err) {
-  dmma_body<BM, true>(&pm, jobs, njobs, ntiles, err);
+                     GemmList *list, unsigned *err) {
+  dmma_body<BM, true>(&pm, jobs, njobs, ntiles, list, err);
 }
 
 template <int BM>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
-    gemm_dmma_kernel_dm(const GemmJob *__restrict__ jobs,
-                        const GemmList *__restrict__ list, unsigned *err) {
-  dmma_body<BM, false>(nullptr, jobs, list->njobs, list->ntiles, err);
+    gemm_dmma_kernel_dm(const GemmJob *__restrict__ jobs, GemmList *list,
+                        unsigned *err) {
+  dmma_body<BM, false>(nullptr, jobs, list->njobs, list->ntiles, list, err);
 }
 
 template <int BM>
-cudaError_t launch(const GemmJob *d_jobs, const GemmList *d_list, int njobs,
+cudaError_t launch(const GemmJob *d_jobs, GemmList *d_list, int njobs,
                    int ntiles, const LaunchMaps *pm, int grid, unsigned *d_err,
                    cudaStream_t st) {
   static bool configured = false;
@@ -252,7 +270,8 @@ cudaError_t launch(const GemmJob *d_jobs, const GemmList *d_list, int njobs,
   }
   if (pm)
     gemm_dmma_kernel<BM><<<grid, GEMM_THREADS, smem, st>>>(*pm, d_jobs, njobs,
-                                                           ntiles, d_err);
+                                                           ntiles, d_list,
+                                                           d_err);
   else
     gemm_dmma_kernel_dm<BM><<<grid, GEMM_THREADS, smem, st>>>(d_jobs, d_list,
                                                               d_err);
@@ -263,10 +282,10 @@ cudaError_t launch(const GemmJob *d_jobs, const GemmList *d_list, int njobs,
 
 size_t gemm_smem_bytes(int bm) {
   return (size_t)ST * (bm * BK + BK * BN) * sizeof(double) +
-         2 * ST * sizeof(uint64_t);
+         2 * ST * sizeof(uint64_t) + sizeof(TileRing);
 }
 
-cudaError_t gemm_dmma_launch(const GemmJob *d_jobs, const GemmList *d_list,
+cudaError_t gemm_dmma_launch(const GemmJob *d_jobs, GemmList *d_list,
                              int njobs, int ntiles, const LaunchMaps *pm,
                              int bm, int grid, unsigned *d_err,
                              cudaStream_t st) {

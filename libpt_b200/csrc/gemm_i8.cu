@@ -203,19 +203,43 @@ __device__ __forceinline__ void i8_drain(const GemmJob &job, int m0, int n0,
   const int erow = rok ? job.ea[row] : 0;
   const uint32_t tbase = tmem + ((uint32_t)(32 * q) << 16);
   constexpr int STEP = 16 * I8_EPI_GROUPS;
-  if (16 * grp >= BN) release();   // no chunk for this warp
-#pragma unroll 1
-  for (int c0 = 16 * grp; c0 < BN; c0 += STEP) {
-    // exact: acc_0..acc_{H-1} and acc_H..acc_{S-1} folded by Horner in base
-    // 2^b into 64-bit integers; |acc| < 2^31 and each sum has at most 4
-    // terms of base 2^7 or 3 of base 2^8 (8-bit digits only for S <= 6), so
-    // |sum| < 2^53 and its conversion to double is exact
-    long long hi[16], lo[16];
-    {
-      uint32_t r[H][16];
+  // chunks a warp drains at most
+  constexpr int NCH = (BN / 16 + I8_EPI_GROUPS - 1) / I8_EPI_GROUPS;
+  {
+    // Each chunk is drained with one TMEM wait (S <= 5: all S loads at
+    // once; else the hi and lo halves, a wait each, to bound the
+    // registers); the chunks' column exponents are loaded before the first
+    // TMEM load (one aligned 16-byte load each: the exponent arrays carry
+    // 16 bytes of padding past their N entries); a chunk's stores are
+    // issued before the next chunk's loads (its registers free), and the
+    // release comes right after the last chunk's loads, before its scaling
+    // and stores.  The fold is exact: acc_0..acc_{H-1} and acc_H..acc_{S-1}
+    // by Horner in base 2^b into 64-bit integers; |acc| < 2^31 and each sum
+    // has at most 4 terms of base 2^7 or 3 of base 2^8 (8-bit digits only
+    // for S <= 6), so |sum| < 2^53 and its conversion to double is exact;
+    // one rounding (the fma), then exact power-of-two scales.
+    int4 ebv[NCH];
 #pragma unroll
-      for (int a = 0; a < H; ++a) tmem_ld16(tbase + a * BN + c0, r[a]);
-      tmem_wait_ld();
+    for (int i = 0; i < NCH; ++i) {
+      const int c0 = 16 * grp + i * STEP;
+      ebv[i] = (c0 < BN && rok && n0 + c0 < N)
+                   ? *reinterpret_cast<const int4 *>(eb + n0 + c0)
+                   : make_int4(0, 0, 0, 0);
+    }
+    double v[16];
+    // one chunk's S accumulators folded into its rounded pre-scale values
+    auto fold = [&](int c0, double (&vv)[16], bool onewait) {
+      long long hi[16];
+      uint32_t r[S][16];
+      if (onewait) {
+#pragma unroll
+        for (int a = 0; a < S; ++a) tmem_ld16(tbase + a * BN + c0, r[a]);
+        tmem_wait_ld();
+      } else {
+#pragma unroll
+        for (int a = 0; a < H; ++a) tmem_ld16(tbase + a * BN + c0, r[a]);
+        tmem_wait_ld();
+      }
 #pragma unroll
       for (int x = 0; x < 16; ++x) {
         long long h = (int)r[0][x];
@@ -223,38 +247,40 @@ __device__ __forceinline__ void i8_drain(const GemmJob &job, int m0, int n0,
         for (int a = 1; a < H; ++a) h = h * base + (int)r[a][x];
         hi[x] = h;
       }
-    }
-    {
-      uint32_t r[S - H][16];
+      if (!onewait) {
 #pragma unroll
-      for (int a = H; a < S; ++a) tmem_ld16(tbase + a * BN + c0, r[a - H]);
-      tmem_wait_ld();
+        for (int a = H; a < S; ++a) tmem_ld16(tbase + a * BN + c0, r[a]);
+        tmem_wait_ld();
+      }
 #pragma unroll
       for (int x = 0; x < 16; ++x) {
-        long long l = (int)r[0][x];
+        long long l = (int)r[H][x];
 #pragma unroll
-        for (int a = H + 1; a < S; ++a) l = l * base + (int)r[a - H][x];
-        lo[x] = l;
+        for (int a = H + 1; a < S; ++a) l = l * base + (int)r[a][x];
+        vv[x] = fma((double)hi[x], w_hi, (double)l * w_lo);
       }
-    }
-    if (c0 + STEP >= BN) release();   // warp-uniform: the last chunk
-    if (rok && n0 + c0 < N) {
-      // the chunk's 16 column exponents in one aligned 16-byte load (the
-      // exponent arrays carry 16 bytes of padding past their N entries)
-      const int4 ebv = *reinterpret_cast<const int4 *>(eb + n0 + c0);
-      const signed char *eb16 = reinterpret_cast<const signed char *>(&ebv);
+    };
+    // chunks of this warp (warp-uniform)
+    int nch = 0;
+#pragma unroll
+    for (int i = 0; i < NCH; ++i)
+      if (16 * grp + i * STEP < BN) nch = i + 1;
+    if (nch == 0) release();
+#pragma unroll
+    for (int i = 0; i < NCH; ++i) {
+      if (i >= nch) break;
+      const int c0 = 16 * grp + i * STEP;
+      fold(c0, v, S <= 5);
+      if (i == nch - 1) release();   // this thread's TMEM loads are done
+      if (!rok || n0 + c0 >= N) continue;
+      const signed char *eb16 = reinterpret_cast<const signed char *>(&ebv[i]);
 #pragma unroll
       for (int x = 0; x < 16; x += 2) {
         const int col = n0 + c0 + x;
-        if (col < N) {
-          // one rounding, then exact power-of-two scales
-          const double v0 = fma((double)hi[x], w_hi, (double)lo[x] * w_lo) *
-                            pow2i(erow + eb16[x]);
-          const double v1 =
-              fma((double)hi[x + 1], w_hi, (double)lo[x + 1] * w_lo) *
-              pow2i(erow + eb16[x + 1]);
-          *reinterpret_cast<double2 *>(orow + col) = make_double2(v0, v1);
-        }
+        if (col < N)
+          *reinterpret_cast<double2 *>(orow + col) =
+              make_double2(v[x] * pow2i(erow + eb16[x]),
+                           v[x + 1] * pow2i(erow + eb16[x + 1]));
       }
     }
   }
@@ -264,7 +290,7 @@ template <int S, int BN, bool PM, bool TS>
 __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
                                         const GemmJob *__restrict__ jobs,
                                         const int njobs, const int ntiles,
-                                        unsigned *err) {
+                                        GemmList *list, unsigned *err) {
   using C = I8Cfg<S, BN, TS, false>;
   constexpr int ST = C::ST;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -275,7 +301,11 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
   uint64_t *accfull = empty + ST;
   uint64_t *accempty = accfull + 1;
   uint64_t *regbar = accempty + 1;   // TS: A region r free again (2)
-  uint32_t *taddr_s = reinterpret_cast<uint32_t *>(regbar + 2);
+  // the tile queue's ring: read by the MMA thread and the epilogue warps
+  TileRing *tq = reinterpret_cast<TileRing *>(regbar + 2);
+  uint32_t *taddr_s = reinterpret_cast<uint32_t *>(tq + 1);
+  static_assert((2 * ST + 4) * 8 + sizeof(TileRing) + 4 <= 256,
+                "barriers, tile ring and TMEM address fit their 256 bytes");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -287,6 +317,7 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
     mbar_init(accempty, I8_EPI_THREADS);
     mbar_init(&regbar[0], 1);
     mbar_init(&regbar[1], 1);
+    tq_init(tq, 1 + I8_EPI_THREADS / 32);   // MMA thread + epilogue warps
     mbar_fence_init();
   }
   if (warp == 1) {
@@ -306,8 +337,17 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
     int stage = 0;
     uint32_t phase = 0;
     bool ok = true;
+    int qslot = 0;
+    uint32_t qph = 0;
     MapSource<PM> ms(pm);
-    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    // tiles from the launch's queue; the next one is taken while the
+    // current one is staged
+    int tile = tq_take(list);
+    while (ok) {
+      if (!tq_put(tq, qslot, qph, tile < ntiles ? tile : -1, err) ||
+          tile >= ntiles)
+        break;
+      const int next_tile = tq_take(list);
       // job fields are copied to registers: the asm memory clobbers and
       // global stores below would otherwise force reloads
       const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
@@ -340,7 +380,9 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
           }
         }
       }
+      tile = next_tile;
     }
+    tq_finish(list);
   } else if (warp == 1 && lane == 0) {
     // ---------------- MMA issuer ----------------
     int stage = 0;
@@ -348,8 +390,11 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
     bool ok = true;
     int it = 0;
     int t = 0;   // TS: MMA K steps issued (region t & 1)
-    for (int tile = blockIdx.x; tile < ntiles && ok;
-         tile += gridDim.x, ++it) {
+    int qslot = 0;
+    uint32_t qph = 0;
+    for (;; ++it) {
+      const int tile = tq_get(tq, qslot, qph, err, false);
+      if (tile < 0) break;
       const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
       if (!mbar_wait(accempty, (uint32_t)((it & 1) ^ 1), err)) {
         ok = false;
@@ -435,12 +480,16 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
           }
         }
       }
-      if (ok) tc_commit(accfull);
+      if (!ok) break;
+      tc_commit(accfull);
     }
   } else if (warp >= 2) {
     // ---------------- epilogue ----------------
-    int it = 0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    int qslot = 0;
+    uint32_t qph = 0;
+    for (int it = 0;; ++it) {
+      const int tile = tq_get(tq, qslot, qph, err, true);
+      if (tile < 0) break;
       const GemmJob &job = jobs[find_entry(jobs, njobs, tile, &GemmJob::tile_begin)];
       const int local = tile - job.tile_begin;
       if (!mbar_wait(accfull, (uint32_t)(it & 1), err)) break;
@@ -674,15 +723,16 @@ template <int S, int BN, bool TS>
 __global__ void __launch_bounds__(I8_THREADS, 1)
     gemm_i8_kernel(const __grid_constant__ LaunchMaps pm,
                    const GemmJob *__restrict__ jobs, int njobs, int ntiles,
-                   unsigned *err) {
-  i8_body<S, BN, true, TS>(&pm, jobs, njobs, ntiles, err);
+                   GemmList *list, unsigned *err) {
+  i8_body<S, BN, true, TS>(&pm, jobs, njobs, ntiles, list, err);
 }
 
 template <int S, int BN, bool TS>
 __global__ void __launch_bounds__(I8_THREADS, 1)
-    gemm_i8_kernel_dm(const GemmJob *__restrict__ jobs,
-                      const GemmList *__restrict__ list, unsigned *err) {
-  i8_body<S, BN, false, TS>(nullptr, jobs, list->njobs, list->ntiles, err);
+    gemm_i8_kernel_dm(const GemmJob *__restrict__ jobs, GemmList *list,
+                      unsigned *err) {
+  i8_body<S, BN, false, TS>(nullptr, jobs, list->njobs, list->ntiles, list,
+                            err);
 }
 
 template <int S, int BN>
@@ -713,7 +763,7 @@ cudaError_t configure(K1 k1, K2 k2, int smem, bool &done) {
 }
 
 template <int S, int BN, bool TS>
-cudaError_t launch(const GemmJob *d_jobs, const GemmList *d_list, int njobs,
+cudaError_t launch(const GemmJob *d_jobs, GemmList *d_list, int njobs,
                    int ntiles, const LaunchMaps *pm, int grid, unsigned *d_err,
                    cudaStream_t st) {
   using C = I8Cfg<S, BN, TS, false>;
@@ -724,7 +774,7 @@ cudaError_t launch(const GemmJob *d_jobs, const GemmList *d_list, int njobs,
     return e;
   if (pm)
     gemm_i8_kernel<S, BN, TS><<<grid, I8_THREADS, C::SMEM, st>>>(
-        *pm, d_jobs, njobs, ntiles, d_err);
+        *pm, d_jobs, njobs, ntiles, d_list, d_err);
   else
     gemm_i8_kernel_dm<S, BN, TS><<<grid, I8_THREADS, C::SMEM, st>>>(
         d_jobs, d_list, d_err);
@@ -778,7 +828,7 @@ int i8_tiles(int slices, const I8Tile **out) {
 }
 
 cudaError_t gemm_i8_launch(int slices, I8Tile t, const GemmJob *d_jobs,
-                           const GemmList *d_list, int njobs, int ntiles,
+                           GemmList *d_list, int njobs, int ntiles,
                            const LaunchMaps *pm, int grid, unsigned *d_err,
                            cudaStream_t st) {
   if (grid <= 0) return cudaSuccess;

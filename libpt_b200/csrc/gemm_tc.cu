@@ -341,7 +341,7 @@ cudaError_t launch(const GemmJob *d_jobs, const GemmList *d_list, int njobs,
 
 int tc_kchunk_elems(int kind) { return kind == TC_TF32 ? 32 : 0; }
 
-cudaError_t gemm_tc_launch(const GemmJob *d_jobs, const GemmList *d_list,
+cudaError_t gemm_tc_launch(const GemmJob *d_jobs, GemmList *d_list,
                            int njobs, int ntiles, const LaunchMaps *pm,
                            int grid, const TcProducts &prods, unsigned *d_err,
                            cudaStream_t st) {

@@ -152,7 +152,7 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
     job.map0 = 0;
     job.tile_begin = 0;
     std::memcpy(&pm_host, maps, bytes < sizeof(pm_host) ? bytes : sizeof(pm_host));
-    GemmList l;
+    GemmList l{};
     l.jobs = dj;
     l.njobs = 1;
     l.ntiles = job.mtiles * job.ntiles_n;
@@ -330,6 +330,25 @@ int kernel_case(int precision, int m, int n, int k, int reps, double *rel_err,
     if (herr) {
       set_error("libpt_kernel_bench: a device-side wait exceeded its limit");
       return done(LIBPT_ERR_TIMEOUT);
+    }
+    // the launches reuse one work list, whose tile queue each launch must
+    // leave reset for the next: one more launch into a cleared output has
+    // to reproduce the first launch's result bit for bit (each element is
+    // accumulated in a fixed order by whichever CTA takes its tile)
+    cudaMemset(Cm, 0, (size_t)m * np * 8);
+    ce = launch();
+    if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
+    std::vector<double> h2((size_t)m * np);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpy(h2.data(), Cm, h2.size() * 8, cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) {
+      set_error(std::string("libpt_kernel_bench: ") + cudaGetErrorString(ce));
+      return done(LIBPT_ERR_CUDA);
+    }
+    if (std::memcmp(h2.data(), hm.data(), h2.size() * 8) != 0) {
+      set_error("libpt_kernel_bench: a relaunch of the same work list gave a "
+                "different result");
+      return done(LIBPT_ERR_CUDA);
     }
   }
   return done(LIBPT_OK);

@@ -12,9 +12,9 @@
 //   runner    builds a round from the resident solves (least remaining work
 //             first, up to a flop budget, at most one round in flight per
 //             solve since a solve's round workspace is reused), launches it
-//             on the run stream -- replaying the captured CUDA graph of the
-//             round's kernel variants when the round is small, direct
-//             launches with parameter-table tensor maps otherwise -- and
+//             on the run stream by replaying the CUDA graph captured for
+//             the round's set of kernel variants (the first round of a set
+//             launches directly, then captures) -- and
 //             retires finished rounds; a solve whose triples have all run
 //             has its energy read back (queue-order compensated sum) and
 //             its block returned to the pool.
@@ -121,10 +121,13 @@ struct RoundRec {
   std::vector<std::shared_ptr<Solve>> solves;
 };
 
-// Round sizing: the flops of one round (about 50 ms of FP64 work), rounds
-// below GRAPH_FLOPS replay graphs, and the round workspace a solve gets.
+// Round sizing: the flops of one round (about 50 ms of FP64 work) and the
+// round workspace a solve gets.  Every round replays a captured graph: the
+// kernels read their tensor maps from device memory there, which measured
+// as fast as the kernel-parameter maps of direct launches (FP64 DMMA and
+// every INT8 tile variant within 1 %, 477 x 65536 x 477 jobs), so the
+// graphs cost large rounds nothing and save small rounds their launches.
 constexpr double ROUND_FLOPS = 1.5e12;
-constexpr double GRAPH_FLOPS = 5e10;
 constexpr size_t ROUND_TRIPLES = 8192;
 constexpr size_t JOBS_PER_TRIPLE = 6;
 constexpr size_t WS_TARGET = (size_t)4 << 30;   // per round, per solve
@@ -444,7 +447,7 @@ void run_loop(libpt_server *S) {
       std::lock_guard<std::mutex> lk(S->mu);
       for (auto &s : rr.solves) ++s->inflight;
     }
-    const bool replay = round.gemm_flops < GRAPH_FLOPS;
+    const bool replay = true;
     const int64_t replays0 = S->exec.graph_replays();
     int64_t launches = 0;
     int r = S->exec.run(round, S->d_err, nullptr, &launches, replay);

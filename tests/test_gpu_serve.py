@@ -116,3 +116,21 @@ def test_small_rounds_replay_graphs():
     assert st["graph_rounds"] >= 1
     for c, e in zip(cases, es):
         assert e == solo(c, 0)
+
+
+def test_large_rounds_replay_graphs():
+    """Rounds of any size replay the graph of their variant set: every round
+    but the first of each set is a replay, and the energies stay those of
+    the plans alone."""
+    # three solves of one size (one variant set), ~3.9e12 flops each: more
+    # than two rounds each at the server's 1.5e12-flop rounds
+    cases = [synth.rpt_case(12, 150, seed=40 + i) for i in range(3)]
+    srv = ffi.Server(mem_budget=32 << 30, max_active=1)
+    ts = [srv.submit(c) for c in cases]
+    es = [srv.wait(t)[0] for t in ts]
+    st = srv.stats()
+    srv.close()
+    assert st["rounds"] >= 6
+    assert st["graph_rounds"] >= st["rounds"] - 1
+    for c, e in zip(cases, es):
+        assert e == solo(c, 0)
