@@ -33,6 +33,18 @@ namespace {
 // in flight than two (31 -> 40 % of DRAM peak measured), four spill.
 constexpr int EPI_MINB = 3;
 
+// Shared-memory layout (doubles) of the mixed-spin epilogue's staged
+// disconnected-term slices, after its U2 / P staging: g1[j,k][b][c],
+// g1[i,k][b][c] (EPI_B x EPI_C each), g1[j,i][b][a] (EPI_B x EPI_A), t1[i][b],
+// t1[j][b], d[j][b] (EPI_B each), then the same for the f_ov half.
+constexpr int EPI_SD_G1JK = 0, EPI_SD_G1IK = 256, EPI_SD_G1JI = 512,
+              EPI_SD_T1I = 576, EPI_SD_T1J = 584, EPI_SD_DJ = 592,
+              EPI_SD_G2JK = 600, EPI_SD_G2IK = 856, EPI_SD_G2JI = 1112,
+              EPI_SD_F1I = 1176, EPI_SD_F1J = 1184, EPI_SD_SIZE = 1192;
+static_assert(EPI_THREADS == EPI_B * EPI_C && EPI_B * EPI_C == 256 &&
+                  EPI_A * EPI_B == 64 && EPI_A == 8 && EPI_B == 8,
+              "one staged (b, c) per thread; offsets above");
+
 __device__ __forceinline__ int64_t pairidx(int p, int q) {
   return (int64_t)p * (p - 1) / 2 + q;
 }
@@ -293,6 +305,44 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
   const double *g2ik = p.g2_ab + ((int64_t)i * ob + k) * va * p.g2_ld_ab;
   const double *g2ji = p.g2_aa + ((int64_t)j * oa + i) * va * p.g2_ld_aa;
   const double *u1 = p.ov1_a, *u2 = p.ov2_a;
+  // The parts of the disconnected term that vary with b -- g[b][c] rows,
+  // g[b][a], and the per-b amplitudes and denominators -- are the same for
+  // every warp (a) of the tile: staged once into shared memory (zero where
+  // b or c is outside the space; those elements are masked) instead of
+  // loaded by each warp in the b loop.
+  double *sd = sm + (FT ? 6 : 3) * S;
+  {
+    const int t = threadIdx.x;   // one (b, c) per thread
+    const int bt = b0 + (t >> 5), ct = c0 + (t & 31);
+    const bool okbc = bt < va && ct < vb;
+    cp_async8(&sd[EPI_SD_G1JK + t], g1jk + (okbc ? bt * g1lab + ct : 0), okbc);
+    cp_async8(&sd[EPI_SD_G1IK + t], g1ik + (okbc ? bt * g1lab + ct : 0), okbc);
+    if (has_f) {
+      cp_async8(&sd[EPI_SD_G2JK + t], g2jk + (okbc ? bt * g2lab + ct : 0),
+                okbc);
+      cp_async8(&sd[EPI_SD_G2IK + t], g2ik + (okbc ? bt * g2lab + ct : 0),
+                okbc);
+    }
+    if (t < EPI_B * EPI_A) {   // (b, a) of g[j][i]
+      const int bb = b0 + (t >> 3), aa = a0 + (t & 7);
+      const bool okba = bb < va && aa < va;
+      cp_async8(&sd[EPI_SD_G1JI + t], g1ji + (okba ? bb * g1laa + aa : 0),
+                okba);
+      if (has_f)
+        cp_async8(&sd[EPI_SD_G2JI + t], g2ji + (okba ? bb * g2laa + aa : 0),
+                  okba);
+    } else if (t < EPI_B * EPI_A + EPI_B) {   // per b
+      const int b_ = t - EPI_B * EPI_A, bb = b0 + b_;
+      const bool okb = bb < va;
+      cp_async8(&sd[EPI_SD_T1I + b_], u1 + (okb ? i * va + bb : 0), okb);
+      cp_async8(&sd[EPI_SD_T1J + b_], u1 + (okb ? j * va + bb : 0), okb);
+      cp_async8(&sd[EPI_SD_DJ + b_], p.d_a + (okb ? j * va + bb : 0), okb);
+      if (has_f) {
+        cp_async8(&sd[EPI_SD_F1I + b_], u2 + (okb ? i * va + bb : 0), okb);
+        cp_async8(&sd[EPI_SD_F1J + b_], u2 + (okb ? j * va + bb : 0), okb);
+      }
+    }
+  }
   const int64_t ac1 = (int64_t)ac * p.g1_ld_ab + cc,
                 ac2 = (int64_t)ac * p.g2_ld_ab + cc;
   const double A1jk = g1jk[ac1], A1ik = g1ik[ac1];
@@ -328,14 +378,15 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
     const double rr = FT ? U1r[u_ab] + sx[3 * S + ix] - U1r[u_ba] -
                                sy[3 * S + iy] + sp[3 * S + ix]
                          : w;
-    const int bc1 = bc * g1lab + cc, bc2 = bc * g2lab + cc;
-    double x =
-        t1ia * g1jk[bc1] - u1[i * va + bc] * A1jk - t1ja * g1ik[bc1] +
-        u1[j * va + bc] * A1ik + o1k * g1ji[bc * g1laa + ac];
+    const int bcl = b_ * EPI_C + lane, ba = b_ * EPI_A + a_;
+    double x = t1ia * sd[EPI_SD_G1JK + bcl] - sd[EPI_SD_T1I + b_] * A1jk -
+               t1ja * sd[EPI_SD_G1IK + bcl] + sd[EPI_SD_T1J + b_] * A1ik +
+               o1k * sd[EPI_SD_G1JI + ba];
     if (has_f)   // the (f_ov, t2) half, zero when f_ov is
-      x += f_ia * g2jk[bc2] - u2[i * va + bc] * A2jk - f_ja * g2ik[bc2] +
-           u2[j * va + bc] * A2ik + o2k * g2ji[bc * g2laa + ac];
-    const double dd = (dia + p.d_a[j * va + bc]) + dkc;
+      x += f_ia * sd[EPI_SD_G2JK + bcl] - sd[EPI_SD_F1I + b_] * A2jk -
+           f_ja * sd[EPI_SD_G2IK + bcl] + sd[EPI_SD_F1J + b_] * A2ik +
+           o2k * sd[EPI_SD_G2JI + ba];
+    const double dd = (dia + sd[EPI_SD_DJ + b_]) + dkc;
     if (ok) e += (w - x) * rr / dd;
   }
   const double s = block_sum(e);
@@ -385,7 +436,8 @@ cudaError_t launch_epi(K kern, const EpiList *d_list, size_t smem, dim3 grid,
 
 size_t epi_smem_bytes(bool aab, bool ft) {
   const size_t s = (size_t)EPI_A * EPI_B * EPI_CS * sizeof(double);
-  return (aab ? 3 : 1) * (ft ? 2 : 1) * s;
+  return (aab ? 3 : 1) * (ft ? 2 : 1) * s +
+         (aab ? EPI_SD_SIZE * sizeof(double) : 0);
 }
 
 int epi_blocks_per_sm(bool aab, bool ft) {

@@ -176,6 +176,8 @@ struct I8Cfg {
 constexpr int I8_EPI_GROUPS = 3;
 constexpr int I8_EPI_THREADS = 4 * I8_EPI_GROUPS * 32;
 constexpr int I8_THREADS = 64 + I8_EPI_THREADS;   // producer, MMA, epilogue
+// (14 warps: four of them on some SM sub-partition, whose 16K registers cap
+// the kernels at 128 registers per thread.)
 
 // Drains one tile's accumulators (this CTA's 128 rows, rows from m0): the
 // S INT32 sums of each element folded exactly, rounded once, scaled and
@@ -226,38 +228,82 @@ __device__ __forceinline__ void i8_drain(const GemmJob &job, int m0, int n0,
                    ? *reinterpret_cast<const int4 *>(eb + n0 + c0)
                    : make_int4(0, 0, 0, 0);
     }
-    double v[16];
-    // one chunk's S accumulators folded into its rounded pre-scale values
-    auto fold = [&](int c0, double (&vv)[16], bool onewait) {
-      long long hi[16];
+    // one chunk's S accumulators folded into its rounded pre-scale values:
+    // all S loads and one wait, or (fewer registers) the hi and lo halves
+    // with a wait each
+    auto fold_one = [&](int c0, double (&vv)[16]) {
       uint32_t r[S][16];
-      if (onewait) {
 #pragma unroll
-        for (int a = 0; a < S; ++a) tmem_ld16(tbase + a * BN + c0, r[a]);
-        tmem_wait_ld();
-      } else {
-#pragma unroll
-        for (int a = 0; a < H; ++a) tmem_ld16(tbase + a * BN + c0, r[a]);
-        tmem_wait_ld();
-      }
+      for (int a = 0; a < S; ++a) tmem_ld16(tbase + a * BN + c0, r[a]);
+      tmem_wait_ld();
 #pragma unroll
       for (int x = 0; x < 16; ++x) {
         long long h = (int)r[0][x];
 #pragma unroll
         for (int a = 1; a < H; ++a) h = h * base + (int)r[a][x];
-        hi[x] = h;
-      }
-      if (!onewait) {
-#pragma unroll
-        for (int a = H; a < S; ++a) tmem_ld16(tbase + a * BN + c0, r[a]);
-        tmem_wait_ld();
-      }
-#pragma unroll
-      for (int x = 0; x < 16; ++x) {
         long long l = (int)r[H][x];
 #pragma unroll
         for (int a = H + 1; a < S; ++a) l = l * base + (int)r[a][x];
+        vv[x] = fma((double)h, w_hi, (double)l * w_lo);
+      }
+    };
+    auto fold_split = [&](int c0, double (&vv)[16]) {
+      long long hi[16];
+      {
+        uint32_t r[H][16];
+#pragma unroll
+        for (int a = 0; a < H; ++a) tmem_ld16(tbase + a * BN + c0, r[a]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int x = 0; x < 16; ++x) {
+          long long h = (int)r[0][x];
+#pragma unroll
+          for (int a = 1; a < H; ++a) h = h * base + (int)r[a][x];
+          hi[x] = h;
+        }
+      }
+      uint32_t r[S - H][16];
+#pragma unroll
+      for (int a = H; a < S; ++a) tmem_ld16(tbase + a * BN + c0, r[a - H]);
+      tmem_wait_ld();
+#pragma unroll
+      for (int x = 0; x < 16; ++x) {
+        long long l = (int)r[0][x];
+#pragma unroll
+        for (int a = H + 1; a < S; ++a) l = l * base + (int)r[a - H][x];
         vv[x] = fma((double)hi[x], w_hi, (double)l * w_lo);
+      }
+    };
+    // stores of one chunk: 32-byte vectors (a full sector per row) where
+    // the output's alignment allows, else 16-byte pairs
+    const bool v4 = ((job.ldc & 3) == 0) &&
+                    ((reinterpret_cast<uintptr_t>(job.out) & 31) == 0);
+    auto store = [&](int i, const double (&vv)[16]) {
+      const int c0 = 16 * grp + i * STEP;
+      if (!rok || n0 + c0 >= N) return;
+      const signed char *eb16 = reinterpret_cast<const signed char *>(&ebv[i]);
+      if (v4) {   // N % 4 == 0: a group of four columns is whole
+#pragma unroll
+        for (int x = 0; x < 16; x += 4) {
+          const int col = n0 + c0 + x;
+          if (col < N)
+            asm volatile(
+                "st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(orow + col),
+                "d"(vv[x] * pow2i(erow + eb16[x])),
+                "d"(vv[x + 1] * pow2i(erow + eb16[x + 1])),
+                "d"(vv[x + 2] * pow2i(erow + eb16[x + 2])),
+                "d"(vv[x + 3] * pow2i(erow + eb16[x + 3]))
+                : "memory");
+        }
+      } else {
+#pragma unroll
+        for (int x = 0; x < 16; x += 2) {
+          const int col = n0 + c0 + x;
+          if (col < N)
+            *reinterpret_cast<double2 *>(orow + col) =
+                make_double2(vv[x] * pow2i(erow + eb16[x]),
+                             vv[x + 1] * pow2i(erow + eb16[x + 1]));
+        }
       }
     };
     // chunks of this warp (warp-uniform)
@@ -266,21 +312,30 @@ __device__ __forceinline__ void i8_drain(const GemmJob &job, int m0, int n0,
     for (int i = 0; i < NCH; ++i)
       if (16 * grp + i * STEP < BN) nch = i + 1;
     if (nch == 0) release();
+    // all chunks but the last two: fold and store in turn; the last two are
+    // both folded before the release and stored after it, so that no store
+    // (32 rows of scattered sectors per instruction) delays the release
+    double v[16], w[16];
 #pragma unroll
     for (int i = 0; i < NCH; ++i) {
       if (i >= nch) break;
       const int c0 = 16 * grp + i * STEP;
-      fold(c0, v, S <= 5);
-      if (i == nch - 1) release();   // this thread's TMEM loads are done
-      if (!rok || n0 + c0 >= N) continue;
-      const signed char *eb16 = reinterpret_cast<const signed char *>(&ebv[i]);
-#pragma unroll
-      for (int x = 0; x < 16; x += 2) {
-        const int col = n0 + c0 + x;
-        if (col < N)
-          *reinterpret_cast<double2 *>(orow + col) =
-              make_double2(v[x] * pow2i(erow + eb16[x]),
-                           v[x + 1] * pow2i(erow + eb16[x + 1]));
+      if (i + 2 < nch) {
+        if constexpr (S <= 5) fold_one(c0, v); else fold_split(c0, v);
+        store(i, v);
+      } else if (i + 2 == nch) {
+        if constexpr (S <= 5) fold_one(c0, v); else fold_split(c0, v);
+      } else {   // the last chunk
+        if (i == 0) {
+          if constexpr (S <= 5) fold_one(c0, v); else fold_split(c0, v);
+          release();   // this thread's TMEM loads are done
+          store(i, v);
+        } else {
+          fold_split(c0, w);
+          release();
+          store(i - 1, v);
+          store(i, w);
+        }
       }
     }
   }

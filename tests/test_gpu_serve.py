@@ -131,6 +131,9 @@ def test_large_rounds_replay_graphs():
     st = srv.stats()
     srv.close()
     assert st["rounds"] >= 6
-    assert st["graph_rounds"] >= st["rounds"] - 1
+    # a variant set is the GEMM variants plus which energy kernels run (the
+    # same-spin triples come first in a queue, so a solve's rounds see a few
+    # sets); only the first round of each set launches directly
+    assert st["graph_rounds"] >= st["rounds"] - 4, st
     for c, e in zip(cases, es):
         assert e == solo(c, 0)

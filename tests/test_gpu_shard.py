@@ -1,8 +1,9 @@
 """A solve sharded over ranks, on one GPU: the ranks' runs are emulated one
 after another on one plan (no kernel waits on another), their slot arrays
 summed as the all-reduce would, and the energy compared bitwise with the
-unsharded solve; then a one-rank NCCL group runs the whole sharded path
-(libpt_b200.shard) through a real all-reduce."""
+unsharded solve and, for the FP64 cases, with the oracle directly; then a
+one-rank NCCL group runs the whole sharded path (libpt_b200.shard) through a
+real all-reduce, checked against the oracle as well."""
 import datetime
 import os
 import socket
@@ -10,7 +11,8 @@ import socket
 import pytest
 
 from libpt_b200 import ffi, synth
-from tests.test_gpu_parity import to_dev
+from oracle import oracle
+from tests.test_gpu_parity import checker, close64, to_dev
 
 pytestmark = pytest.mark.gpu
 
@@ -44,7 +46,10 @@ def test_emulated_ranks_give_the_unsharded_energy(kind, sz, prec, size):
             acc += own
         plan.energy_slots().copy_(acc)
         torch.cuda.synchronize()
-        assert plan.energy() == whole
+        sharded = plan.energy()
+        assert sharded == whole
+        if prec == ffi.PREC_FP64:
+            assert close64(sharded, oracle.solve(checker(), case))
     finally:
         plan.close()
 
@@ -65,5 +70,6 @@ def test_one_rank_nccl_group_runs_the_sharded_path():
         case = synth.make("rpt", 6, 20, seed=9, fock=1e-3)
         e = shard.solve_sharded(case, to_dev(case))
         assert e == ffi.solve_host(case)
+        assert close64(e, oracle.solve(checker(), case))
     finally:
         dist.destroy_process_group()
