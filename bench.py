@@ -124,8 +124,8 @@ PRECISIONS = {"fp64": 0, "tf32x3": 1, "emu64": 2}
 # profiles/gemm_i8_rpt_o2_v477_emu64s5_full.txt).  A launch's traffic grows
 # with its triples (each reads its own operand slices and writes its own
 # outputs), so the bench scales these by the flops of its launches.
-DRAM_BYTES_PER_FLOP = {"gemm_dmma_kernel": (7.141e9 + 4.338e9) / 9.26e11,
-                       "gemm_i8_kernel": (11.637e9 + 4.342e9) / 9.26e11}
+DRAM_BYTES_PER_FLOP = {"gemm_dmma_kernel": (7.022e9 + 4.340e9) / 9.26e11,
+                       "gemm_i8_kernel": (5.281e9 + 4.353e9) / 9.26e11}
 
 
 # ------------------------------------------------------------------ helpers
@@ -685,6 +685,65 @@ def serve_stream(n, rate, seed):
     return reqs
 
 
+def rpt_lengths(o, v):
+    """Element counts of the pt.h restricted (T) arrays (src/pt.h:26-62):
+    t2 and i_oovv hold the aaaa and abab blocks, i_oovo likewise, i_ovvv
+    the packed aaaa block (pairs b > c) then the abab block."""
+    ov = o * v
+    return dict(d_ov=ov, f_ov=ov, t1=ov, t2=2 * o * o * v * v,
+                i_oovo=2 * o * o * o * v, i_oovv=2 * o * o * v * v,
+                i_ovvv=ov * (v * (v - 1) // 2) + ov * v * v)
+
+
+def serve_inputs(reqs, torch):
+    """Host arrays of every request of the served stream.  t1, f_ov (zero)
+    and d_ov (e_i - e_a, e_i ~ U[-1.5, -0.3], e_a ~ U[0.1, 3.0]) are each
+    request's own; its four large arrays are windows, at offsets drawn from
+    its seed, into two shared host pools of normal deviates (std 1e-2 for
+    t2, 5e-2 for the integrals: the synthetic configs' distributions,
+    without their permutational symmetries, on which neither the work nor
+    its speed depends).  Own symmetric inputs for every request average
+    ~1.1 GiB (o ~ U{4..24}, v ~ o * U[6, 12]): 300 requests would need
+    ~325 GiB of host memory.  Returns (cases, pooled GiB, GiB the requests
+    would hold on their own)."""
+    big = ("t2", "i_oovo", "i_oovv", "i_ovvv")
+    lens = [rpt_lengths(r["o"], r["v"]) for r in reqs]
+    slack = 1 << 24                              # room for distinct offsets
+    n_amp = max(x["t2"] for x in lens) + slack
+    n_int = max(max(x[k] for k in big[1:]) for x in lens) + slack
+
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+
+    def pool(n, std, seed):
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed)
+        out = np.empty(n, dtype=np.float64)
+        step = 1 << 27
+        for a in range(0, n, step):              # 1 GiB pieces
+            b = min(n, a + step)
+            out[a:b] = torch.randn(b - a, generator=g, dtype=torch.float64,
+                                   device=dev).mul_(std).cpu().numpy()
+        return out
+
+    amp, integ = pool(n_amp, 1e-2, 71), pool(n_int, 5e-2, 72)
+    cases = []
+    for r, ln in zip(reqs, lens):
+        rng = np.random.default_rng(r["seed"])
+        o, v = r["o"], r["v"]
+        e_i = rng.uniform(-1.5, -0.3, o)
+        e_a = rng.uniform(0.1, 3.0, v)
+        case = dict(kind="rpt", oa=o, va=v, ob=o, vb=v,
+                    d_ov=(e_i[:, None] - e_a[None, :]).reshape(-1),
+                    f_ov=np.zeros(o * v), t1=rng.normal(0.0, 1e-3, o * v))
+        for k in big:
+            src = amp if k == "t2" else integ
+            at = int(rng.integers(0, (src.size - ln[k]) // 512 + 1)) * 512
+            case[k] = src[at:at + ln[k]]
+        cases.append(case)
+    own = sum(sum(x.values()) for x in lens) * 8 / 2**30
+    return cases, (amp.nbytes + integ.nbytes) / 2**30, own
+
+
 def percentile(x, q):
     return float(np.percentile(np.asarray(x), q)) if len(x) else None
 
@@ -707,22 +766,13 @@ def run_serving(args, torch, gpu_id):
     one-at-a-time FP64 solves through libpt_rpt (host arrays), FIFO at the
     same arrivals: service times measured once, queueing computed per
     rate."""
-    from libpt_b200 import ffi, synth
+    from libpt_b200 import ffi
     rates = [float(x) for x in args.serve_rates.split(",") if x]
     reqs = serve_stream(args.serve_requests, 1.0, seed=4)   # unit rate
     emu = ffi.PREC_EMU64 | (args.serve_slices << 8)
     t_prep = time.perf_counter()
-    cases = []
-    for r in reqs:
-        meta, tens = synth.rpt_case_device(r["o"], r["v"], seed=r["seed"])
-        case = dict(meta)
-        case.update({k: t.cpu().numpy() for k, t in tens.items()})
-        del tens
-        cases.append(case)
-    torch.cuda.empty_cache()
+    cases, host_gb, own_gb = serve_inputs(reqs, torch)
     t_prep = time.perf_counter() - t_prep
-    host_gb = sum(sum(a.nbytes for k, a in c.items()
-                      if isinstance(a, np.ndarray)) for c in cases) / 2**30
     budget = int(args.serve_budget_gb * (1 << 30))
     budget = min(budget, int(torch.cuda.mem_get_info()[0] - (8 << 30)))
     flops = sum(rpt_flops(r["o"], r["v"]) for r in reqs)
@@ -781,8 +831,10 @@ def run_serving(args, torch, gpu_id):
                  "emulated FP64 (slices "
                  + ("chosen for 1 uEh" if args.serve_slices == 0 else
                     f"fixed at {args.serve_slices}")
-                 + f"), host inputs ({host_gb:.1f} GiB, prepared in "
-                 f"{t_prep:.0f} s before the streams)",
+                 + f"), host inputs prepared in {t_prep:.0f} s before the "
+                 f"streams: each request's large arrays are windows into "
+                 f"{host_gb:.1f} GiB of shared pools of the synthetic "
+                 f"distributions ({own_gb:.0f} GiB on their own)",
         flops=flops, pool_gb=budget / 2**30,
         sustainable_solves_per_s=max(r["solves_per_s"] for r in per_rate),
         sustainable_note="the highest throughput measured: every rate "

@@ -181,6 +181,14 @@ int libpt_kernel_bench(int precision, int m, int n, int k, int reps,
  * counterpart in the reference. */
 int libpt_selftest_wait(int stages, int arrive, double limit_ms, int *seen);
 
+/* Accuracy of the energy epilogues' reciprocal of the denominators (an
+ * approximate reciprocal refined by two Newton-Raphson steps, used in place
+ * of a division): *max_ulp = the largest distance, in units in the last
+ * place, from the IEEE division 1.0 / d over n values d = +-m * 2^x, x in
+ * [lo_exp, hi_exp] (-1000 <= lo_exp <= hi_exp <= 1000), m in [1, 2).  No
+ * counterpart in the reference (its energy divides, src/pt.c:291-295). */
+int libpt_selftest_recip(int lo_exp, int hi_exp, int n, double *max_ulp);
+
 /* ---- device-pointer twins ----------------------------------------------
  * Same arguments as the reference entry points, but every tensor is a
  * device pointer on the current device and `stream` (a cudaStream_t, may be

@@ -247,6 +247,24 @@ __device__ __forceinline__ int find_entry(const T *v, int n, int x,
   return lo;
 }
 
+// 1/d for the energy denominators (normal doubles with 2^-1000 <= |d| <=
+// 2^1000), within 2 ulp of the correctly rounded reciprocal
+// (libpt_selftest_recip measures it against IEEE division):
+// the hardware's approximate reciprocal (PTX rcp.approx.ftz.f64, about 20
+// correct bits) refined by two Newton-Raphson steps r <- r + r (1 - d r),
+// each of which squares the relative error.  The energy epilogues multiply
+// by it instead of dividing (an element's energy carries a few more
+// rounding errors of 2^-53), in place of the much longer IEEE division
+// sequence in kernels whose instruction issue is one of their limits.
+__device__ __forceinline__ double recip_nr(double d) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+
 // ---- device-resident tile queue ---------------------------------------------
 //
 // The reference hands triples to OpenMP threads one at a time

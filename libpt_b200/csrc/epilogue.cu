@@ -89,6 +89,24 @@ __device__ __forceinline__ void cp_async_wait_all() {
                    : "memory");
 }
 
+// A persistent CTA's walk over the items of an EpiList, kept in shared
+// memory (no registers live across tiles): its tiles come in increasing
+// order and an item spans many of them, so the binary search (a chain of
+// dependent global loads) runs only when a tile leaves the current item, and
+// the case arguments are copied to shared memory only when they change
+// (items of one spin case of one plan share them).  Thread 0 advances it
+// before the barrier that ends a tile.
+struct ItemWalk {
+  int cur, next_begin;          // item index; first tile of the next item
+  const EpiArgs *staged;        // whose arguments shared memory holds
+  __device__ __forceinline__ void seek(const EpiList *l, int blk) {
+    if (blk < next_begin) return;
+    cur = find_entry(l->items, l->nitems, blk, &EpiItem::block_begin);
+    next_begin = cur + 1 < l->nitems ? l->items[cur + 1].block_begin
+                                     : 0x7fffffff;
+  }
+};
+
 // Copies an item's case arguments into shared memory (all threads).
 __device__ __forceinline__ void load_args(EpiArgs &dst, const EpiArgs *src) {
   static_assert(sizeof(EpiArgs) % 8 == 0, "8-byte words");
@@ -112,14 +130,23 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
   // CTA per (tile, item) of a 2-D grid
   int blk = blockIdx.x;
   if (LOOP && blk >= list->nblocks) return;
+  __shared__ ItemWalk walk;
+  if (LOOP) {
+    if (threadIdx.x == 0) {
+      walk.next_begin = 0;
+      walk.staged = nullptr;
+      walk.seek(list, blk);
+    }
+    __syncthreads();
+  }
   do {
-  const EpiItem &item =
-      LOOP ? list->items[find_entry(list->items, list->nitems, blk,
-                                    &EpiItem::block_begin)]
-           : list->items[blockIdx.y];
+  const EpiItem &item = list->items[LOOP ? walk.cur : blockIdx.y];
   const int local = LOOP ? blk - item.block_begin : blk;
   if (!LOOP && local >= item.nblk) return;
-  load_args(p, item.args);
+  if (!LOOP || item.args != walk.staged) {   // uniform over the CTA
+    load_args(p, item.args);   // ends with a barrier
+    if (LOOP && threadIdx.x == 0) walk.staged = item.args;
+  }
   const int4 tl = p.tiles[local];
   const int a0 = tl.x, b0 = tl.y, c0 = tl.z;
   const int i = item.i, j = item.j, k = item.k;
@@ -206,13 +233,14 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
            u2[k * v + bc] * A2ji - f_ic * g2jk[ba2] + f_jc * g2ik[ba2] +
            f_kc * g2ji[ba2];
     const double dd = (dia + p.d_a[j * v + bc]) + dkc;
-    if (ok) e += (w - x) * rr / dd;
+    if (ok) e += (w - x) * rr * recip_nr(dd);
   }
   const double s = block_sum(e);
   if (threadIdx.x == 0) item.partials[local] = s;
   if (!LOOP) break;
-  __syncthreads();   // shared memory is refilled by the next tile
   blk += gridDim.x;
+  if (threadIdx.x == 0) walk.seek(list, blk);
+  __syncthreads();   // shared memory is refilled by the next tile
   } while (blk < list->nblocks);
 }
 
@@ -232,14 +260,23 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
   // CTA per (tile, item) of a 2-D grid
   int blk = blockIdx.x;
   if (LOOP && blk >= list->nblocks) return;
+  __shared__ ItemWalk walk;
+  if (LOOP) {
+    if (threadIdx.x == 0) {
+      walk.next_begin = 0;
+      walk.staged = nullptr;
+      walk.seek(list, blk);
+    }
+    __syncthreads();
+  }
   do {
-  const EpiItem &item =
-      LOOP ? list->items[find_entry(list->items, list->nitems, blk,
-                                    &EpiItem::block_begin)]
-           : list->items[blockIdx.y];
+  const EpiItem &item = list->items[LOOP ? walk.cur : blockIdx.y];
   const int local = LOOP ? blk - item.block_begin : blk;
   if (!LOOP && local >= item.nblk) return;
-  load_args(p, item.args);
+  if (!LOOP || item.args != walk.staged) {   // uniform over the CTA
+    load_args(p, item.args);   // ends with a barrier
+    if (LOOP && threadIdx.x == 0) walk.staged = item.args;
+  }
   const int npairs = p.ntiles / p.ctiles;   // tiles: c block major
   // the (a, b) tiles are the triangle a0 = 8t, b0 = 8u, u <= t, in row
   // order (the last row may stop at u = t - 1); tile L sits in row
@@ -387,13 +424,14 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
            f_ja * sd[EPI_SD_G2IK + bcl] + sd[EPI_SD_F1J + b_] * A2ik +
            o2k * sd[EPI_SD_G2JI + ba];
     const double dd = (dia + sd[EPI_SD_DJ + b_]) + dkc;
-    if (ok) e += (w - x) * rr / dd;
+    if (ok) e += (w - x) * rr * recip_nr(dd);
   }
   const double s = block_sum(e);
   if (threadIdx.x == 0) item.partials[local] = s;
   if (!LOOP) break;
-  __syncthreads();   // shared memory is refilled by the next tile
   blk += gridDim.x;
+  if (threadIdx.x == 0) walk.seek(list, blk);
+  __syncthreads();   // shared memory is refilled by the next tile
   } while (blk < list->nblocks);
 }
 

@@ -431,6 +431,28 @@ __global__ void wait_probe_kernel(int stages, int arrive,
 
 }  // namespace
 
+// Largest distance in units in the last place between recip_nr(d) and the
+// IEEE division 1.0 / d over n values d = +-2^x, x evenly spaced in
+// [lo_exp, hi_exp], times a mantissa that walks [1, 2).
+__global__ void recip_probe_kernel(int lo_exp, int hi_exp, int n,
+                                   unsigned long long *worst) {
+  unsigned long long w = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    const double f = n > 1 ? (double)i / (double)(n - 1) : 0.0;
+    const double x = lo_exp + f * (double)(hi_exp - lo_exp);
+    const double m = 1.0 + (double)((i * 2654435761u) >> 8) * 0x1p-24;
+    double d = ldexp(m, (int)floor(x));
+    if (i & 1) d = -d;
+    const long long a = __double_as_longlong(ptb::recip_nr(d));
+    const long long b = __double_as_longlong(1.0 / d);
+    const unsigned long long u =
+        (unsigned long long)(a > b ? a - b : b - a);   // same sign: ulps
+    w = u > w ? u : w;
+  }
+  atomicMax(worst, w);
+}
+
 LIBPT_API int libpt_selftest_wait(int stages, int arrive, double limit_ms,
                                   int *seen) {
   if (stages < 1 || stages > 4096 || arrive < 0 || arrive > stages ||
@@ -461,5 +483,31 @@ LIBPT_API int libpt_selftest_wait(int stages, int arrive, double limit_ms,
                    "time limit of " + std::to_string(limit_ms) + " ms");
     return LIBPT_ERR_TIMEOUT;
   }
+  return LIBPT_OK;
+}
+
+LIBPT_API int libpt_selftest_recip(int lo_exp, int hi_exp, int n,
+                                   double *max_ulp) {
+  if (lo_exp < -1000 || hi_exp > 1000 || lo_exp > hi_exp || n < 1 ||
+      n > (1 << 28) || !max_ulp) {
+    ptb::set_error("libpt_selftest_recip: bad arguments");
+    return LIBPT_ERR_ARG;
+  }
+  unsigned long long *buf = nullptr;
+  CK(cudaMalloc(&buf, sizeof(*buf)));
+  cudaError_t ce = cudaMemset(buf, 0, sizeof(*buf));
+  if (ce == cudaSuccess) {
+    recip_probe_kernel<<<148 * 4, 256>>>(lo_exp, hi_exp, n, buf);
+    ce = cudaGetLastError();
+  }
+  if (ce == cudaSuccess) ce = cudaDeviceSynchronize();
+  unsigned long long h = 0;
+  if (ce == cudaSuccess) ce = cudaMemcpy(&h, buf, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(buf);
+  if (ce != cudaSuccess) {
+    ptb::set_error(std::string("libpt_selftest_recip: ") + cudaGetErrorString(ce));
+    return LIBPT_ERR_CUDA;
+  }
+  *max_ulp = (double)h;
   return LIBPT_OK;
 }

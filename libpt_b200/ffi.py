@@ -102,6 +102,9 @@ def lib():
     L.libpt_selftest_wait.argtypes = [ctypes.c_int, ctypes.c_int,
                                       ctypes.c_double,
                                       ctypes.POINTER(ctypes.c_int)]
+    L.libpt_selftest_recip.restype = ctypes.c_int
+    L.libpt_selftest_recip.argtypes = [ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, dp]
     # serving (pt_serve.h)
     L.libpt_footprint.restype = sz
     L.libpt_footprint.argtypes = [ctypes.c_int] + [sz] * 4 + [ctypes.c_int] * 3 + [sz]
@@ -213,6 +216,15 @@ def selftest_wait(stages, arrive, limit_ms):
     code = lib().libpt_selftest_wait(stages, arrive, limit_ms,
                                      ctypes.byref(seen))
     return code, seen.value
+
+
+def selftest_recip(lo_exp, hi_exp, n):
+    """Largest distance in ulps between the energy epilogues' reciprocal and
+    the IEEE division 1.0 / d over n values d = +-m 2^x, x in [lo_exp,
+    hi_exp] (libpt_selftest_recip)."""
+    worst = ctypes.c_double(-1.0)
+    check(lib().libpt_selftest_recip(lo_exp, hi_exp, n, ctypes.byref(worst)))
+    return worst.value
 
 
 HOST_MALLOC = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_size_t)

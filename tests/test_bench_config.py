@@ -103,3 +103,23 @@ def test_precision_cases_have_reference_energies():
         assert r["kind"] == kind and tuple(r["sizes"]) == sz
         assert r["seed"] == seed
         assert r["fp64"]["energy"] != 0.0 and r["fp32_mp"]["energy"] != 0.0
+
+
+def test_served_inputs_are_windows_of_the_pt_h_sizes():
+    """Every request of the served stream gets arrays of the pt.h lengths
+    (those of synth.rpt_case), its large ones inside the shared pools, and
+    two requests of one size get different windows."""
+    import numpy as np
+    import torch
+    from libpt_b200 import synth
+    reqs = [dict(o=3, v=20, seed=1), dict(o=3, v=20, seed=2),
+            dict(o=4, v=31, seed=3)]
+    cases, pool_gb, own_gb = bench.serve_inputs(reqs, torch)
+    for r, c in zip(reqs, cases):
+        ref = synth.rpt_case(r["o"], r["v"], seed=0)
+        for k, n in bench.rpt_lengths(r["o"], r["v"]).items():
+            assert c[k].size == ref[k].size == n, k
+            assert c[k].dtype == np.float64 and c[k].flags.c_contiguous
+        assert (c["d_ov"] < 0).all()
+    assert not np.array_equal(cases[0]["i_ovvv"], cases[1]["i_ovvv"])
+    assert pool_gb > own_gb

@@ -73,3 +73,18 @@ def test_device_memory_tensor_maps(m, n, k):
         assert ffi.selftest(prec, m, n, k, 0, device_maps=True) < EMU_BOUND[s]
         assert ffi.selftest(prec, m, n, k, 0, device_maps=True,
                             dbits=8) < EMU8_BOUND[s]
+
+
+@pytest.mark.parametrize("lo,hi", [(-10, 10), (-1000, 1000)])
+def test_energy_reciprocal_is_within_two_ulp_of_division(lo, hi):
+    """The energy epilogues multiply by a Newton-refined reciprocal of the
+    denominator instead of dividing: within 2 ulp of IEEE 1.0 / d over the
+    range their docs state (the (T) denominators lie near 2^-3..2^5)."""
+    assert ffi.selftest_recip(lo, hi, 1 << 22) <= 2.0
+
+
+def test_energy_reciprocal_rejects_bad_ranges():
+    with pytest.raises(ffi.LibptError):
+        ffi.selftest_recip(-1001, 0, 16)
+    with pytest.raises(ffi.LibptError):
+        ffi.selftest_recip(3, 2, 16)
