@@ -221,11 +221,15 @@ struct RedList {
 size_t epi_smem_bytes(bool aab, bool ft);
 // persistent: `grid` CTAs stride over list->nblocks tiles (a fixed grid,
 // for graph replay); otherwise a (max tiles of an item) x (items) grid, one
-// CTA per tile, grid = max tiles and nitems the item count.
-cudaError_t epi_aaa_launch(const EpiList *d_list, bool ft, bool hasf, int grid,
-                           int nitems, bool persistent, cudaStream_t st);
-cudaError_t epi_aab_launch(const EpiList *d_list, bool ft, bool hasf, int grid,
-                           int nitems, bool persistent, cudaStream_t st);
+// CTA per tile, grid = max tiles and nitems the item count, whose CTAs read
+// their item from d_items (the list's item array, passed directly so that
+// the tile's first load does not wait for the list).
+cudaError_t epi_aaa_launch(const EpiList *d_list, const EpiItem *d_items,
+                           bool ft, bool hasf, int grid, int nitems,
+                           bool persistent, cudaStream_t st);
+cudaError_t epi_aab_launch(const EpiList *d_list, const EpiItem *d_items,
+                           bool ft, bool hasf, int grid, int nitems,
+                           bool persistent, cudaStream_t st);
 // CTAs the epilogue keeps resident per SM (for persistent grids).
 int epi_blocks_per_sm(bool aab, bool ft);
 cudaError_t reduce_partials_launch(const RedList *d_list, int grid,

@@ -119,7 +119,8 @@ __device__ __forceinline__ void load_args(EpiArgs &dst, const EpiArgs *src) {
 
 template <bool FT, bool LOOP, bool HASF>
 __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
-    epi_aaa_kernel(const EpiList *__restrict__ list) {
+    epi_aaa_kernel(const EpiList *__restrict__ list,
+                   const EpiItem *__restrict__ items) {
   extern __shared__ double sm[];
   __shared__ EpiArgs p;
   constexpr int S = EPI_A * EPI_B * EPI_CS;
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
     __syncthreads();
   }
   do {
-  const EpiItem &item = list->items[LOOP ? walk.cur : blockIdx.y];
+  const EpiItem &item = LOOP ? list->items[walk.cur] : items[blockIdx.y];
   const int local = LOOP ? blk - item.block_begin : blk;
   if (!LOOP && local >= item.nblk) return;
   if (!LOOP || item.args != walk.staged) {   // uniform over the CTA
@@ -248,7 +249,8 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
 
 template <bool FT, bool LOOP, bool HASF>
 __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
-    epi_aab_kernel(const EpiList *__restrict__ list) {
+    epi_aab_kernel(const EpiList *__restrict__ list,
+                   const EpiItem *__restrict__ items) {
   extern __shared__ double sm[];
   __shared__ EpiArgs p;
   constexpr int S = EPI_A * EPI_B * EPI_CS;
@@ -270,7 +272,7 @@ __global__ void __launch_bounds__(EPI_THREADS, EPI_MINB)
     __syncthreads();
   }
   do {
-  const EpiItem &item = list->items[LOOP ? walk.cur : blockIdx.y];
+  const EpiItem &item = LOOP ? list->items[walk.cur] : items[blockIdx.y];
   const int local = LOOP ? blk - item.block_begin : blk;
   if (!LOOP && local >= item.nblk) return;
   if (!LOOP || item.args != walk.staged) {   // uniform over the CTA
@@ -462,11 +464,11 @@ cudaError_t set_smem(K kern, size_t bytes) {
 }
 
 template <typename K>
-cudaError_t launch_epi(K kern, const EpiList *d_list, size_t smem, dim3 grid,
-                       cudaStream_t st) {
+cudaError_t launch_epi(K kern, const EpiList *d_list, const EpiItem *d_items,
+                       size_t smem, dim3 grid, cudaStream_t st) {
   cudaError_t e = set_smem(kern, smem);
   if (e != cudaSuccess) return e;
-  kern<<<grid, EPI_THREADS, smem, st>>>(d_list);
+  kern<<<grid, EPI_THREADS, smem, st>>>(d_list, d_items);
   return cudaGetLastError();
 }
 
@@ -509,34 +511,38 @@ int epi_blocks_per_sm(bool aab, bool ft) {
 // Persistent launches (fixed grids, graph replays) use the general kernels;
 // direct launches whose items all have a zero f_ov (hasf false) use the
 // kernels compiled without the f_ov terms.
-cudaError_t epi_aaa_launch(const EpiList *d_list, bool ft, bool hasf, int grid,
-                           int nitems, bool persistent, cudaStream_t st) {
+cudaError_t epi_aaa_launch(const EpiList *d_list, const EpiItem *d_items,
+                           bool ft, bool hasf, int grid, int nitems,
+                           bool persistent, cudaStream_t st) {
   if (grid <= 0 || nitems <= 0) return cudaSuccess;
+  if (!persistent && !d_items) return cudaErrorInvalidValue;
   const size_t smem = epi_smem_bytes(false, ft);
   const dim3 g(grid, persistent ? 1 : nitems);
   if (persistent)
-    return ft ? launch_epi(epi_aaa_kernel<true, true, true>, d_list, smem, g, st)
-              : launch_epi(epi_aaa_kernel<false, true, true>, d_list, smem, g, st);
+    return ft ? launch_epi(epi_aaa_kernel<true, true, true>, d_list, d_items, smem, g, st)
+              : launch_epi(epi_aaa_kernel<false, true, true>, d_list, d_items, smem, g, st);
   if (hasf)
-    return ft ? launch_epi(epi_aaa_kernel<true, false, true>, d_list, smem, g, st)
-              : launch_epi(epi_aaa_kernel<false, false, true>, d_list, smem, g, st);
-  return ft ? launch_epi(epi_aaa_kernel<true, false, false>, d_list, smem, g, st)
-            : launch_epi(epi_aaa_kernel<false, false, false>, d_list, smem, g, st);
+    return ft ? launch_epi(epi_aaa_kernel<true, false, true>, d_list, d_items, smem, g, st)
+              : launch_epi(epi_aaa_kernel<false, false, true>, d_list, d_items, smem, g, st);
+  return ft ? launch_epi(epi_aaa_kernel<true, false, false>, d_list, d_items, smem, g, st)
+            : launch_epi(epi_aaa_kernel<false, false, false>, d_list, d_items, smem, g, st);
 }
 
-cudaError_t epi_aab_launch(const EpiList *d_list, bool ft, bool hasf, int grid,
-                           int nitems, bool persistent, cudaStream_t st) {
+cudaError_t epi_aab_launch(const EpiList *d_list, const EpiItem *d_items,
+                           bool ft, bool hasf, int grid, int nitems,
+                           bool persistent, cudaStream_t st) {
   if (grid <= 0 || nitems <= 0) return cudaSuccess;
+  if (!persistent && !d_items) return cudaErrorInvalidValue;
   const size_t smem = epi_smem_bytes(true, ft);
   const dim3 g(grid, persistent ? 1 : nitems);
   if (persistent)
-    return ft ? launch_epi(epi_aab_kernel<true, true, true>, d_list, smem, g, st)
-              : launch_epi(epi_aab_kernel<false, true, true>, d_list, smem, g, st);
+    return ft ? launch_epi(epi_aab_kernel<true, true, true>, d_list, d_items, smem, g, st)
+              : launch_epi(epi_aab_kernel<false, true, true>, d_list, d_items, smem, g, st);
   if (hasf)
-    return ft ? launch_epi(epi_aab_kernel<true, false, true>, d_list, smem, g, st)
-              : launch_epi(epi_aab_kernel<false, false, true>, d_list, smem, g, st);
-  return ft ? launch_epi(epi_aab_kernel<true, false, false>, d_list, smem, g, st)
-            : launch_epi(epi_aab_kernel<false, false, false>, d_list, smem, g, st);
+    return ft ? launch_epi(epi_aab_kernel<true, false, true>, d_list, d_items, smem, g, st)
+              : launch_epi(epi_aab_kernel<false, false, true>, d_list, d_items, smem, g, st);
+  return ft ? launch_epi(epi_aab_kernel<true, false, false>, d_list, d_items, smem, g, st)
+            : launch_epi(epi_aab_kernel<false, false, false>, d_list, d_items, smem, g, st);
 }
 
 cudaError_t reduce_partials_launch(const RedList *d_list, int grid,

@@ -200,8 +200,9 @@ int Executor::launch_all(const std::vector<GemmGroup> &groups,
       }
       if (grid <= 0) continue;
       const bool hasf = fixed || r->epi_hasf[a][f];
-      CK(a ? epi_aab_launch(lst, f, hasf, grid, nitems, fixed, st_)
-           : epi_aaa_launch(lst, f, hasf, grid, nitems, fixed, st_));
+      const EpiItem *items = fixed ? nullptr : epi_items_[a][f];
+      CK(a ? epi_aab_launch(lst, items, f, hasf, grid, nitems, fixed, st_)
+           : epi_aaa_launch(lst, items, f, hasf, grid, nitems, fixed, st_));
       if (launches) ++*launches;
     }
   {
@@ -303,6 +304,7 @@ int Executor::run(Round &r, unsigned *d_err, ExecTiming *timing,
       std::memcpy(h + eoff[a][f], it.data(), it.size() * sizeof(EpiItem));
       EpiList l;
       l.items = reinterpret_cast<const EpiItem *>(d_buf_ + eoff[a][f]);
+      epi_items_[a][f] = l.items;   // direct launches take it as a parameter
       l.nitems = (int32_t)it.size();
       l.nblocks = it.empty() ? 0
                              : it.back().block_begin + r.epi_blocks[a][f].back();

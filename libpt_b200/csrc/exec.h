@@ -102,6 +102,7 @@ class Executor {
   int64_t replays_ = 0;
   std::vector<const GemmJob *> gjobs_;   // device job arrays of the groups
   int epi_grid_[2][2] = {{0, 0}, {0, 0}};
+  const EpiItem *epi_items_[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
 
 }  // namespace ptb
