@@ -590,11 +590,13 @@ def run_ours(args, d):
                    workload=f"libpt_rpt(o={O_E2E}, v={args.v}) host arrays, "
                             "full solve")
 
+    # the served stream and the precision table are single-GPU reports:
+    # rank 0 runs them (the other ranks' lines are not printed)
     serving = None
-    if args.serve_requests > 0:
+    if args.serve_requests > 0 and d.rank == 0:
         serving = run_serving(args, torch, gpu_id)
     accuracy = None
-    if not args.no_accuracy:
+    if not args.no_accuracy and d.rank == 0:
         accuracy = run_accuracy(args, torch)
 
     cpu = None
