@@ -15,8 +15,8 @@ time is the queue's flops over that rate.
 Lines printed (rank 0, one JSON line):
   value      whole-job TFLOP/s, device-resident operands, CUDA-event timed
   e2e        libpt_rpt (host arrays, the reference-facing C ABI) on a full
-             solve of o=4, v=477 with the host->device copies inside the
-             timed region
+             solve of o=8, v=477 (10.6 GB of host arrays, 280 triples) with
+             the host->device copies inside the timed region
   roofline   the contraction kernel (gemm_dmma_kernel): achieved FP64 TFLOP/s
              from CUDA events around each launch over the measured FP64
              tensor peak (cuBLAS DGEMM measured here, MEASURED_PEAKS.json
@@ -61,7 +61,7 @@ if ROOT not in sys.path:
 
 O_FULL, V_FULL = 45, 477      # the workload (restricted, all-electron)
 STRIDE = 211                  # triples-queue sampling stride of one step
-O_E2E = 4                     # full solves through the host API
+O_E2E = 8                     # full solves through the host API
 O_CPU = 0                     # the reference's host sample (0: per kind)
 CPU_FULL_O = 4                # full solve in the reference's own layout
 
@@ -569,8 +569,13 @@ def run_ours(args, d):
     # ---- e2e: reference-facing host API, copies inside the timed region ---
     e2e = None
     if not args.no_e2e:
-        case = synth.rpt_case(O_E2E, args.v, seed=77 + d.rank)
-        arrs = {n: np.ascontiguousarray(case[n]) for n in ffi.PT_ARGS}
+        # inputs generated on the device, then held in host memory as the
+        # caller's arrays (10.6 GB at o=8, v=477)
+        meta, tens = synth.rpt_case_device(O_E2E, args.v, seed=77 + d.rank)
+        case = dict(meta)
+        arrs = {n: tens[n].cpu().numpy() for n in ffi.PT_ARGS}
+        del tens
+        torch.cuda.empty_cache()
         case.update(arrs)
         h2d = sum(a.nbytes for a in arrs.values())
         ffi.solve_host(case)                       # warm-up
