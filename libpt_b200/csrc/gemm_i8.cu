@@ -37,7 +37,9 @@
 //   warp 0      TMA producer: the S A planes and S B planes of one K chunk
 //               per stage
 //   warp 1      TMEM owner and MMA issuer (one thread): S(S+1)/2 products
-//               per K step; tcgen05.commit frees the stage
+//               per K step (one CTA: those of one A plane with up to
+//               256 / BN adjacent B planes merged into one MMA);
+//               tcgen05.commit frees the stage
 //   warps 2-13  epilogue: tcgen05.ld of the S accumulators, combined exactly
 //               in 64-bit integers into two partial sums, one FP64 rounding,
 //               an exact power-of-two scale, FP64 store.  Three warps per
@@ -137,6 +139,12 @@ template <int M, int BN>
 __host__ __device__ constexpr uint32_t i8_idesc() {
   return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
+}
+
+// B planes one MMA of the one-CTA form multiplies at once: N = G * BN <= 256
+// (at most 4, the most any slice count's products need).
+constexpr int i8_group(int bn) {
+  return 256 / bn > 4 ? 4 : (256 / bn < 1 ? 1 : 256 / bn);
 }
 
 constexpr int pow2_cols(int c) {
@@ -512,17 +520,37 @@ __device__ __forceinline__ void i8_body(const LaunchMaps *pm,
               tc_commit(&regbar[r]);
               ++t;
             } else {
+              // A_pa times B_pb .. B_pb+g-1 in one MMA of N = g * BN: the B
+              // planes lie back to back in the stage (same swizzle atoms, so
+              // g planes read as one tile of g * BN rows), and the
+              // accumulators of weights pa + pb .. pa + pb + g - 1 are
+              // adjacent TMEM columns, so column block j of the product
+              // lands in acc_{pa+pb+j}.  A_pa is read once per group
+              // instead of once per product (S = 5, BN = 96: 9 MMAs and 9 A
+              // reads per K step instead of 15).
 #pragma unroll
               for (int pa = 0; pa < S; ++pa) {
                 const uint64_t da =
                     da0 + (uint64_t)((pa * C::A_TILE + kk * 32) >> 4);
 #pragma unroll
-                for (int pb = 0; pb + pa < S; ++pb) {
+                for (int pb = 0; pb + pa < S; pb += i8_group(BN)) {
                   const int w = pa + pb;     // digit weight 2^-b(w+2)
+                  const int g = S - w < i8_group(BN) ? S - w : i8_group(BN);
                   const uint64_t db =
                       db0 + (uint64_t)((pb * C::B_TILE + kk * 32) >> 4);
-                  mma_i8(tmem + (uint32_t)(w * BN), da, db, i8_idesc<BM, BN>(),
-                         (pa > 0 || kk > 0) ? 1u : later);
+                  const uint32_t acc = (pa > 0 || kk > 0) ? 1u : later;
+                  if (g == 4)
+                    mma_i8(tmem + (uint32_t)(w * BN), da, db,
+                           i8_idesc<BM, 4 * BN>(), acc);
+                  else if (g == 3)
+                    mma_i8(tmem + (uint32_t)(w * BN), da, db,
+                           i8_idesc<BM, 3 * BN>(), acc);
+                  else if (g == 2)
+                    mma_i8(tmem + (uint32_t)(w * BN), da, db,
+                           i8_idesc<BM, 2 * BN>(), acc);
+                  else
+                    mma_i8(tmem + (uint32_t)(w * BN), da, db,
+                           i8_idesc<BM, BN>(), acc);
                 }
               }
             }
