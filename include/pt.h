@@ -189,6 +189,23 @@ int libpt_selftest_wait(int stages, int arrive, double limit_ms, int *seen);
  * counterpart in the reference (its energy divides, src/pt.c:291-295). */
 int libpt_selftest_recip(int lo_exp, int hi_exp, int n, double *max_ulp);
 
+/* ---- upstream producer (device) -----------------------------------------
+ * Builds the restricted (T) inputs of libpt_rpt / libpt_rpt_dev on the
+ * device from a density-fitted closed-shell CCSD's results: the
+ * three-index factors b_oo[Q][i][j], b_ov[Q][i][a], b_vv[Q][a][b]
+ * (naux x o x o, naux x o x v, naux x v x v, row-major, device pointers)
+ * give i_oovv abab = (ia|jb), i_ovvv abab = (ib|ac), i_oovo abab = (ia|jk)
+ * and their same-spin (aaaa) blocks in the pt.h layout; t2_abab (o x o x v
+ * x v, may be t2 + o*o*v*v, or NULL to leave t2 alone) gives t2's aaaa and
+ * abab blocks.  Outputs are device arrays of the libpt_rpt sizes.  Work is
+ * ordered on `stream`; the call returns once it is queued (the GEMMs run
+ * through cuBLAS, loaded at the first call).  Returns LIBPT_OK or an error
+ * code.  No counterpart in the reference (its caller builds these arrays). */
+int libpt_rpt_inputs_df(size_t o, size_t v, size_t naux, const double *b_oo,
+    const double *b_ov, const double *b_vv, const double *t2_abab,
+    double *t2, double *i_oovo, double *i_oovv, double *i_ovvv,
+    void *stream);
+
 /* ---- device-pointer twins ----------------------------------------------
  * Same arguments as the reference entry points, but every tensor is a
  * device pointer on the current device and `stream` (a cudaStream_t, may be

@@ -28,7 +28,8 @@ HOST_CXX = "/usr/bin/g++"   # the image's $CXX wrapper lacks some runtime specs
 SOURCES = ["gemm_dmma.cu", "gemm_tc.cu", "gemm_i8.cu", "epilogue.cu", "prep.cu",
            "exec.cu", "plan.cu", "plan_views.cu", "plan_upload.cu",
            "plan_cases.cu", "plan_emu.cu", "plan_tune.cu", "plan_run.cu",
-           "tune.cpp", "api.cpp", "noalloc.cu", "selftest.cu", "server.cpp"]
+           "tune.cpp", "api.cpp", "noalloc.cu", "selftest.cu", "server.cpp",
+           "producer.cu"]
 HEADERS = ["common.cuh", "engine.h", "exec.h", "plan.h", "plan_impl.h",
            "tune.h"]
 

@@ -18,6 +18,7 @@ KINDS = ("rpt", "upt", "rft", "uft")
 KIND_ID = {k: i for i, k in enumerate(KINDS)}
 
 LIBPT_OK = 0
+LIBPT_ERR_ARG = 1
 LIBPT_ERR_NOMEM = 2
 LIBPT_ERR_TIMEOUT = 4
 LIBPT_ERR_CANCELLED = 6
@@ -102,6 +103,8 @@ def lib():
     L.libpt_selftest_wait.argtypes = [ctypes.c_int, ctypes.c_int,
                                       ctypes.c_double,
                                       ctypes.POINTER(ctypes.c_int)]
+    L.libpt_rpt_inputs_df.restype = ctypes.c_int
+    L.libpt_rpt_inputs_df.argtypes = [sz, sz, sz] + [vp] * 8 + [vp]
     L.libpt_selftest_recip.restype = ctypes.c_int
     L.libpt_selftest_recip.argtypes = [ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, dp]
@@ -216,6 +219,32 @@ def selftest_wait(stages, arrive, limit_ms):
     code = lib().libpt_selftest_wait(stages, arrive, limit_ms,
                                      ctypes.byref(seen))
     return code, seen.value
+
+
+def rpt_inputs_df(b_oo, b_ov, b_vv, t2_abab=None, stream=None):
+    """Restricted (T) integral arrays (and t2, when t2_abab is given) in the
+    pt.h layout, built on the device from density-fitted factors
+    (libpt_rpt_inputs_df).  b_oo, b_ov, b_vv: CUDA float64 tensors of shapes
+    (naux, o, o), (naux, o, v), (naux, v, v); t2_abab: (o, o, v, v).  Returns
+    a dict of the produced CUDA tensors by pt.h argument name."""
+    import torch
+    naux, o, v = b_ov.shape
+    f64 = dict(dtype=torch.float64, device=b_ov.device)
+    out = dict(i_oovo=torch.empty(2 * o * o * v * o, **f64),
+               i_oovv=torch.empty(2 * o * o * v * v, **f64),
+               i_ovvv=torch.empty(o * v * (v * (v - 1) // 2) + o * v * v * v,
+                                  **f64))
+    if t2_abab is not None:
+        out["t2"] = torch.empty(2 * o * o * v * v, **f64)
+    ins = [b_oo.contiguous(), b_ov.contiguous(), b_vv.contiguous(),
+           None if t2_abab is None else t2_abab.contiguous()]
+    ptr = lambda t: None if t is None else t.data_ptr()   # noqa: E731
+    check(lib().libpt_rpt_inputs_df(
+        o, v, naux, *[ptr(t) for t in ins], ptr(out.get("t2")),
+        ptr(out["i_oovo"]), ptr(out["i_oovv"]), ptr(out["i_ovvv"]),
+        stream or 0))
+    torch.cuda.synchronize()   # the inputs (and any copies above) stay alive
+    return out
 
 
 def selftest_recip(lo_exp, hi_exp, n):
