@@ -198,9 +198,10 @@ int libpt_selftest_recip(int lo_exp, int hi_exp, int n, double *max_ulp);
  * and their same-spin (aaaa) blocks in the pt.h layout; t2_abab (o x o x v
  * x v, may be t2 + o*o*v*v, or NULL to leave t2 alone) gives t2's aaaa and
  * abab blocks.  Outputs are device arrays of the libpt_rpt sizes.  Work is
- * ordered on `stream`; the call returns once it is queued (the GEMMs run
- * through cuBLAS, loaded at the first call).  Returns LIBPT_OK or an error
- * code.  No counterpart in the reference (its caller builds these arrays). */
+ * ordered on `stream` and may still run when the call returns (the GEMMs run
+ * through cuBLAS, loaded at the first call; a v^3 scratch block is
+ * allocated stream-ordered).  Returns LIBPT_OK or an error code.  No
+ * counterpart in the reference (its caller builds these arrays). */
 int libpt_rpt_inputs_df(size_t o, size_t v, size_t naux, const double *b_oo,
     const double *b_ov, const double *b_vv, const double *t2_abab,
     double *t2, double *i_oovo, double *i_oovv, double *i_ovvv,
