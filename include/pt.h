@@ -207,6 +207,20 @@ int libpt_rpt_inputs_df(size_t o, size_t v, size_t naux, const double *b_oo,
     double *t2, double *i_oovo, double *i_oovv, double *i_ovvv,
     void *stream);
 
+/* The unrestricted (T) integrals of libpt_upt / libpt_upt_dev from the
+ * factors of each spin (b_*_a: alpha, oa x va; b_*_b: beta, ob x vb; same
+ * layouts as above): abab blocks (ia|jb), (ib|ac), (ia|jk) with the first
+ * occupied and first virtual index alpha, baba the same with the spins
+ * exchanged, aaaa / bbbb the antisymmetrised same-spin products.  The
+ * amplitudes, spin blocks of their own in an unrestricted CCSD, are not
+ * touched.  A factor array with no elements (o or v zero) may be NULL.
+ * Same ordering and allocation as libpt_rpt_inputs_df. */
+int libpt_upt_inputs_df(size_t oa, size_t va, size_t ob, size_t vb,
+    size_t naux, const double *b_oo_a, const double *b_ov_a,
+    const double *b_vv_a, const double *b_oo_b, const double *b_ov_b,
+    const double *b_vv_b, double *i_oovo, double *i_oovv, double *i_ovvv,
+    void *stream);
+
 /* ---- device-pointer twins ----------------------------------------------
  * Same arguments as the reference entry points, but every tensor is a
  * device pointer on the current device and `stream` (a cudaStream_t, may be

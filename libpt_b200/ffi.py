@@ -105,6 +105,8 @@ def lib():
                                       ctypes.POINTER(ctypes.c_int)]
     L.libpt_rpt_inputs_df.restype = ctypes.c_int
     L.libpt_rpt_inputs_df.argtypes = [sz, sz, sz] + [vp] * 8 + [vp]
+    L.libpt_upt_inputs_df.restype = ctypes.c_int
+    L.libpt_upt_inputs_df.argtypes = [sz] * 5 + [vp] * 9 + [vp]
     L.libpt_selftest_recip.restype = ctypes.c_int
     L.libpt_selftest_recip.argtypes = [ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, dp]
@@ -243,6 +245,32 @@ def rpt_inputs_df(b_oo, b_ov, b_vv, t2_abab=None, stream=None):
         o, v, naux, *[ptr(t) for t in ins], ptr(out.get("t2")),
         ptr(out["i_oovo"]), ptr(out["i_oovv"]), ptr(out["i_ovvv"]),
         stream or 0))
+    torch.cuda.synchronize()   # the inputs (and any copies above) stay alive
+    return out
+
+
+def upt_inputs_df(fa, fb, stream=None):
+    """Unrestricted (T) integral arrays in the pt.h layout built on the
+    device (libpt_upt_inputs_df) from each spin's factors fa, fb = (b_oo,
+    b_ov, b_vv) CUDA float64 tensors of shapes (naux, o, o), (naux, o, v),
+    (naux, v, v).  Returns a dict of the produced CUDA tensors."""
+    import torch
+    naux, oa, va = fa[1].shape
+    ob, vb = fb[1].shape[1:]
+    npa, npb = va * (va - 1) // 2, vb * (vb - 1) // 2
+    f64 = dict(dtype=torch.float64, device=fa[1].device)
+    out = dict(
+        i_oovo=torch.empty(oa * oa * va * oa + oa * ob * va * ob +
+                           ob * ob * vb * ob + ob * oa * vb * oa, **f64),
+        i_oovv=torch.empty(oa * oa * va * va + 2 * oa * ob * va * vb +
+                           ob * ob * vb * vb, **f64),
+        i_ovvv=torch.empty(oa * va * npa + oa * vb * va * vb + ob * vb * npb +
+                           ob * va * vb * va, **f64))
+    ins = [t.contiguous() for t in (*fa, *fb)]
+    check(lib().libpt_upt_inputs_df(
+        oa, va, ob, vb, naux, *[t.data_ptr() for t in ins],
+        out["i_oovo"].data_ptr(), out["i_oovv"].data_ptr(),
+        out["i_ovvv"].data_ptr(), stream or 0))
     torch.cuda.synchronize()   # the inputs (and any copies above) stay alive
     return out
 

@@ -77,3 +77,36 @@ def test_bad_arguments_are_refused():
     assert f(1, 1, 1, None, p, p, None, None, p, p, p, None) == ffi.LIBPT_ERR_ARG
     assert f(70000, 70000, 1, p, p, p, None, None, p, p, p, None) == \
         ffi.LIBPT_ERR_ARG
+
+
+@pytest.mark.parametrize("oa,va,ob,vb,naux", [(3, 5, 2, 6, 7), (1, 1, 1, 2, 2),
+                                              (2, 4, 0, 5, 3), (4, 13, 3, 14, 20),
+                                              (2, 40, 3, 33, 17)])
+def test_unrestricted_arrays_match_the_restatement(oa, va, ob, vb, naux):
+    from tests.test_producer import df_inputs_u, spin_factors
+    fa = spin_factors(oa, va, naux, seed=1)
+    fb = spin_factors(ob, vb, naux, seed=2)
+    got = ffi.upt_inputs_df([to_cuda(x) for x in fa], [to_cuda(x) for x in fb])
+    want = df_inputs_u(fa, fb)
+    for name, ref in want.items():
+        dev = got[name].cpu().numpy()
+        assert dev.shape == ref.shape, name
+        scale = max(np.abs(ref).max() if ref.size else 0.0, 1e-300)
+        assert np.abs(dev - ref).max(initial=0.0) <= 1e-13 * scale, name
+
+
+@pytest.mark.parametrize("oa,va,ob,vb", [(4, 11, 3, 13), (5, 21, 4, 23)])
+def test_unrestricted_solve_of_produced_inputs_matches_the_oracle(oa, va, ob,
+                                                                  vb):
+    from tests.test_producer import df_inputs_u, spin_factors
+    naux = 30
+    fa = spin_factors(oa, va, naux, seed=5)
+    fb = spin_factors(ob, vb, naux, seed=6)
+    case = synth.upt_case(oa, va, ob, vb, seed=oa, fock=1e-3)
+    host = dict(case)
+    host.update(df_inputs_u(fa, fb))
+    dev = {n: to_cuda(host[n]) for n in ("d_ov", "f_ov", "t1", "t2")}
+    dev.update(ffi.upt_inputs_df([to_cuda(x) for x in fa],
+                                 [to_cuda(x) for x in fb]))
+    e = ffi.solve_device(case, dev)
+    assert close64(e, oracle.solve(checker(), host))

@@ -1,6 +1,6 @@
-"""The device producer's conventions (libpt_rpt_inputs_df), pinned on the
-reference's own restricted fixtures, and its numpy restatement (the checker
-of tests/test_gpu_producer.py).
+"""The device producer's conventions (libpt_rpt_inputs_df,
+libpt_upt_inputs_df), pinned on the reference's own fixtures, and its numpy
+restatements (the checkers of tests/test_gpu_producer.py).
 
 pt.h asks only for "properly (anti-)symmetrized" tensors (src/pt.h:37-57).
 The fixtures the reference ships (tests/rpt02.dat, rpt09.dat, converted to
@@ -100,3 +100,83 @@ def test_restatement_builds_that_structure():
                       np.sum(b_ov[q, 1, 3] * b_vv[q, 2, 4]))
     assert np.isclose(b["oovo_ab"][0, 2, 5, 1],
                       np.sum(b_ov[q, 0, 5] * b_oo[q, 2, 1]))
+
+
+def df_inputs_u(fa, fb):
+    """Numpy restatement of libpt_upt_inputs_df: the pt.h unrestricted
+    integral arrays (blocks aaaa, abab, bbbb, baba) from each spin's factors
+    fa, fb = (b_oo, b_ov, b_vv)."""
+    def same(oo, ov, vv):
+        v = ov.shape[2]
+        r, c = np.tril_indices(v, -1)
+        g = np.einsum("qia,qjb->ijab", ov, ov)
+        y = np.einsum("qia,qjk->ijak", ov, oo)
+        z = np.einsum("qib,qac->iabc", ov, vv)
+        return ((g - g.transpose(0, 1, 3, 2)).ravel(),
+                (y - y.transpose(1, 0, 2, 3)).ravel(),
+                (z - z.transpose(0, 1, 3, 2))[:, :, r, c].ravel())
+
+    def mixed(x, y):
+        return (np.einsum("qia,qjb->ijab", x[1], y[1]).ravel(),
+                np.einsum("qia,qjk->ijak", x[1], y[0]).ravel(),
+                np.einsum("qib,qac->iabc", x[1], y[2]).ravel())
+    sa, sb, ab, ba = same(*fa), same(*fb), mixed(fa, fb), mixed(fb, fa)
+    return dict(i_oovv=np.concatenate([sa[0], ab[0], sb[0], ba[0]]),
+                i_oovo=np.concatenate([sa[1], ab[1], sb[1], ba[1]]),
+                i_ovvv=np.concatenate([sa[2], ab[2], sb[2], ba[2]]))
+
+
+def spin_factors(o, v, naux, seed):
+    rng = np.random.default_rng(seed)
+    oo = rng.normal(0, 0.1, (naux, o, o))
+    vv = rng.normal(0, 0.1, (naux, v, v))
+    return (0.5 * (oo + oo.transpose(0, 2, 1)), rng.normal(0, 0.1, (naux, o, v)),
+            0.5 * (vv + vv.transpose(0, 2, 1)))
+
+
+@pytest.mark.parametrize("name", ["upt01", "upt03"])
+def test_unrestricted_fixtures_have_the_produced_structure(name):
+    """abab and baba blocks of the reference's unrestricted fixtures are
+    Mulliken products of the same kind: baba oovv is abab's transpose, the
+    OVVV mixed blocks are symmetric in their two same-spin virtual indices
+    and the OOVO ones in their two same-spin occupied indices."""
+    c = fixtures.load(name)
+    oa, va, ob, vb = (int(c[k]) for k in ("oa", "va", "ob", "vb"))
+    npa, npb = va * (va - 1) // 2, vb * (vb - 1) // 2
+
+    def cut(x, sizes):
+        off = np.cumsum([0] + sizes)
+        return [x[off[n]:off[n + 1]] for n in range(len(sizes))]
+    vv = cut(c["i_oovv"], [oa * oa * va * va, oa * ob * va * vb,
+                           ob * ob * vb * vb, ob * oa * vb * va])
+    ab, ba = vv[1].reshape(oa, ob, va, vb), vv[3].reshape(ob, oa, vb, va)
+    tol = 1e-13 * max(np.abs(ab).max(), 1.0)
+    assert np.abs(ba - ab.transpose(1, 0, 3, 2)).max() <= tol
+    v3 = cut(c["i_ovvv"], [oa * va * npa, oa * vb * va * vb, ob * vb * npb,
+                           ob * va * vb * va])
+    for blk, shape in ((v3[1], (oa, vb, va, vb)), (v3[3], (ob, va, vb, va))):
+        x = blk.reshape(shape)
+        assert np.abs(x - x.transpose(0, 3, 2, 1)).max() <= tol
+    vo = cut(c["i_oovo"], [oa * oa * va * oa, oa * ob * va * ob,
+                           ob * ob * vb * ob, ob * oa * vb * oa])
+    for blk, shape in ((vo[1], (oa, ob, va, ob)), (vo[3], (ob, oa, vb, oa))):
+        x = blk.reshape(shape)
+        assert np.abs(x - x.transpose(0, 3, 2, 1)).max() <= tol
+
+
+def test_unrestricted_restatement_with_equal_spins_is_the_restricted_one():
+    """With the same factors for both spins, the unrestricted arrays are the
+    restricted ones with bbbb = aaaa and baba = abab (the identity the
+    restricted path relies on, src/pt.c:469-473)."""
+    o, v, q = 3, 6, 9
+    f = spin_factors(o, v, q, seed=4)
+    u = df_inputs_u(f, f)
+    r = df_inputs(*f)
+    npr = v * (v - 1) // 2
+    assert np.allclose(u["i_oovv"], np.concatenate([r["i_oovv"], r["i_oovv"]]))
+    assert np.allclose(u["i_oovo"], np.concatenate([r["i_oovo"], r["i_oovo"]]))
+    assert np.allclose(u["i_ovvv"],
+                       np.concatenate([r["i_ovvv"][:o * v * npr],
+                                       r["i_ovvv"][o * v * npr:],
+                                       r["i_ovvv"][:o * v * npr],
+                                       r["i_ovvv"][o * v * npr:]]))
