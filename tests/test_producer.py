@@ -180,3 +180,25 @@ def test_unrestricted_restatement_with_equal_spins_is_the_restricted_one():
                                        r["i_ovvv"][o * v * npr:],
                                        r["i_ovvv"][:o * v * npr],
                                        r["i_ovvv"][o * v * npr:]]))
+
+
+def test_producer_entry_points_refuse_bad_arguments_before_any_device_work():
+    """Argument checks come first (no pointer is dereferenced, no CUDA call
+    made), so they run without a GPU."""
+    from libpt_b200 import ffi
+    L = ffi.lib()
+    p = 4096    # never dereferenced: every call below fails its checks
+    assert L.libpt_rpt_inputs_df(0, 2, 2, p, p, p, None, None, p, p, p,
+                                 None) == ffi.LIBPT_ERR_ARG
+    assert L.libpt_rpt_inputs_df(1, 1, 1, p, p, p, p, None, p, p, p,
+                                 None) == ffi.LIBPT_ERR_ARG
+    assert L.libpt_rpt_inputs_df(70000, 70000, 1, p, p, p, None, None, p, p,
+                                 p, None) == ffi.LIBPT_ERR_ARG
+    # unrestricted: a non-empty factor array may not be NULL
+    assert L.libpt_upt_inputs_df(2, 3, 1, 4, 5, p, p, p, None, p, p, p, p, p,
+                                 None) == ffi.LIBPT_ERR_ARG
+    assert L.libpt_upt_inputs_df(2, 3, 0, 4, 5, p, p, p, None, None, None,
+                                 p, p, p, None) == ffi.LIBPT_ERR_ARG   # b_vv_b
+    assert L.libpt_upt_inputs_df(2, 3, 1, 4, 0, p, p, p, p, p, p, p, p, p,
+                                 None) == ffi.LIBPT_ERR_ARG             # naux 0
+    assert b"libpt_upt_inputs_df" in L.libpt_last_error()
